@@ -1,0 +1,142 @@
+"""ctypes binding of ``libfluid_b200.so`` (C ABI in ``include/fluid_b200.h``).
+
+The product path has no fallback: if the library or a CUDA device is missing,
+the solvers raise instead of computing anything on the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfluid_b200.so")
+
+FS_OK = 0
+FS_ERR_INVALID = 1
+FS_ERR_CUDA = 2
+FS_ERR_CAPACITY = 3
+FS_ERR_NOGRID = 4
+
+FS_STATUS_NONFINITE = 1
+FS_STATUS_GRID_OVERFLOW = 2
+FS_STATUS_BOUNDS = 4
+FS_STATUS_TIMEOUT = 8
+
+STATUS_NAMES = {FS_STATUS_NONFINITE: "NONFINITE", FS_STATUS_GRID_OVERFLOW: "GRID_OVERFLOW",
+                FS_STATUS_BOUNDS: "BOUNDS", FS_STATUS_TIMEOUT: "TIMEOUT"}
+
+P = C.c_void_p
+F = C.c_float
+I32 = C.c_int32
+I64 = C.c_int64
+
+
+class GridConfig(C.Structure):
+    _fields_ = [("dim_x", I32), ("dim_y", I32), ("dim_z", I32), ("rounding", I32)]
+
+
+class Model(C.Structure):
+    _fields_ = [("n", I64), ("n_worlds", I32)] + [(k, P) for k in (
+        "particle_flags", "particle_mask", "particle_world", "particle_mass", "gravity", "rest_density",
+        "surface_tension", "viscosity", "stiffness", "exponent")]
+
+
+class State(C.Structure):
+    _fields_ = [(k, P) for k in (
+        "particle_q", "particle_qd", "rho", "pressure", "factor", "rho_star", "d_rho_dt", "kappa", "kappa_v",
+        "neighbor_count", "v_star", "pbf_lambda", "delta_p")]
+
+
+class WcsphParams(C.Structure):
+    _fields_ = [(k, F) for k in ("dt", "smoothing_length", "particle_radius", "bound_width", "bound_height",
+                                 "bound_length", "boundary_damping")] + [("clamp_negative_pressure", I32)]
+
+
+class DfsphParams(C.Structure):
+    _fields_ = [(k, F) for k in ("dt", "smoothing_length", "particle_radius", "bound_width", "bound_height",
+                                 "bound_length", "boundary_damping")] + [
+        (k, I32) for k in ("max_rho_iterations", "max_vel_iterations", "warm_start", "min_neighbors_for_factor")] + [
+        (k, F) for k in ("eta_density", "eta_divergence", "max_kappa", "max_kappa_v")]
+
+
+class PbfParams(C.Structure):
+    _fields_ = [(k, F) for k in ("dt", "smoothing_length", "particle_radius", "bound_width", "bound_height",
+                                 "bound_length", "boundary_damping", "boundary_epsilon")] + [
+        (k, I32) for k in ("max_iterations", "min_neighbors_for_lambda", "rebuild_grid_each_iteration")] + [
+        (k, F) for k in ("lambda_epsilon", "scorr_k", "scorr_n", "scorr_w_delta_q", "max_delta_position", "xsph_c")]
+
+
+class DfsphInfo(C.Structure):
+    _fields_ = [("rho_iterations", I32), ("vel_iterations", I32), ("density_residual", C.c_double),
+                ("divergence_residual", C.c_double)]
+
+
+# name -> (restype, argtypes); must match include/fluid_b200.h
+SIGNATURES = {
+    "fs_context_create": (C.c_int, [C.POINTER(P), I64, C.POINTER(GridConfig), I32]),
+    "fs_context_destroy": (C.c_int, [P]),
+    "fs_context_capacity": (I64, [P]),
+    "fs_grid_build": (C.c_int, [P, P, I64, F, P]),
+    "fs_grid_tables": (C.c_int, [P, P, P, P, P, P]),
+    "fs_grid_candidates": (C.c_int, [P, P, I64, F, P, P, P, P]),
+    "fs_wcsph_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
+                                   C.POINTER(WcsphParams), P, P]),
+    "fs_dfsph_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
+                                   C.POINTER(DfsphParams), P, P]),
+    "fs_dfsph_info_read": (C.c_int, [P, C.POINTER(DfsphInfo)]),
+    "fs_pbf_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
+                                 C.POINTER(PbfParams), P, P, P]),
+    "fs_wcsph_density": (C.c_int, [P, C.POINTER(Model), P, F, I32, P, P, P]),
+    "fs_wcsph_force_integrate": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
+                                           C.POINTER(WcsphParams), P, P]),
+    "fs_dfsph_density_factor": (C.c_int, [P, C.POINTER(Model), P, F, I32, P, P, P, P]),
+    "fs_dfsph_divergence": (C.c_int, [P, C.POINTER(Model), P, P, F, P, P]),
+    "fs_dfsph_correct": (C.c_int, [P, C.POINTER(Model), P, P, P, P, F, F, P]),
+    "fs_dfsph_residual": (C.c_int, [P, C.POINTER(Model), P, P, P, P]),
+    "fs_pbf_density": (C.c_int, [P, C.POINTER(Model), P, F, P, P]),
+    "fs_pbf_lambda": (C.c_int, [P, C.POINTER(Model), P, C.POINTER(PbfParams), P, P, P, P]),
+    "fs_pbf_delta": (C.c_int, [P, C.POINTER(Model), P, P, C.POINTER(PbfParams), P, P]),
+    "fs_pbf_xsph": (C.c_int, [P, C.POINTER(Model), P, P, P, F, F, P, P]),
+    "fs_status_read": (C.c_int, [P, C.POINTER(C.c_uint32)]),
+    "fs_status_clear": (C.c_int, [P, P]),
+    "fs_last_error_string": (C.c_char_p, []),
+    "fs_version": (C.c_char_p, []),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+class FluidLibraryError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the in-tree CUDA library (built by ``__graft_entry__.build`` /
+    ``python -m fluid_simulation_b200.build``).  Raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise FluidLibraryError(
+                    f"{LIB_PATH} is missing: build it with `python -m fluid_simulation_b200.build`; "
+                    "there is no CPU implementation of the solver kernels")
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != FS_OK:
+        msg = load().fs_last_error_string().decode(errors="replace")
+        raise FluidLibraryError(f"{what}: fluid_b200 error {rc}: {msg}")
+
+
+def status_names(word: int):
+    return [name for bit, name in STATUS_NAMES.items() if word & bit]

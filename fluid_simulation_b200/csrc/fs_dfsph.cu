@@ -1,0 +1,600 @@
+// DFSPH substep on B200 (replaces SolverDFSPH.step, solver_dfsph.py:598-898).
+//
+// The reference reads the residual back to the host once per solver
+// iteration (solver_dfsph.py:733, 849).  Here each iteration is a pair of
+// launches whose decision stays on the device:
+//   rate    : d_rho_dt (+ rho_star) + the candidate kappa of every particle +
+//             a deterministic residual reduction; its last block stores the
+//             residual and sets `done` when it > 0 and residual <= eta
+//   correct : if !done, commit kappa and apply the velocity correction
+// Launches of iterations after the break see `done` and return at once, so
+// the whole step is launch-only (graph capturable) and takes exactly the
+// reference's decisions.
+#include "fs_internal.cuh"
+
+namespace fs {
+
+int reduction_blocks(int64_t n) { return blocks_for(n > 0 ? n : 1); }
+
+// gathers of fs_wcsph.cu reused here
+__global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
+                                const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
+                                float* __restrict__ mv, uint32_t* status);
+__global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
+                              const float* __restrict__ b, float2* __restrict__ out);
+
+namespace {
+
+__global__ void k_gather_scalar(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
+                                float* __restrict__ out, float* __restrict__ copy_to) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int32_t i = perm[s];
+  const float v = a[i];
+  out[s] = v;
+  if (copy_to) copy_to[i] = v;
+}
+
+// compute_density (107-133) + compute_factor_dfsph (137-174), one candidate loop.
+struct DensFactorArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vs;  // .w = mass
+  const float* mv;
+  float h;
+  int min_nb;
+  float* rho;
+  float* factor;
+  int32_t* count;
+  float2* sc2;       // (rho, factor) cell order
+};
+
+__global__ void __launch_bounds__(kBlock) k_density_factor(DensFactorArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const int32_t i = a.g.perm[s];
+  if (!(pf_of(xi) & PF_ACTIVE)) {
+    a.rho[i] = 0.f;
+    a.factor[i] = 0.f;
+    a.count[i] = 0;
+    a.sc2[s] = make_float2(0.f, 0.f);
+    return;
+  }
+  const CubicK K(a.h);
+  const float h2m = a.h * a.h * 1.000002f;
+  float rho = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sq = 0.f;
+  int cnt = 0;
+  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+    const float4 xj = __ldg(a.xs + t);
+    if (!(pf_of(xj) & PF_ACTIVE)) return;
+    cnt += (t != s) ? 1 : 0;  // candidates, no distance test (solver_dfsph.py:163-164)
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r2 = dist2_rn(dx, dy, dz);
+    if (r2 > h2m) return;
+    const float r = sqrtf(r2);
+    rho += __ldg(a.mv + t) * K.w(r);
+    const float gsc = __ldg(&a.vs[t].w) * K.dw_scale(r);
+    const float gx = gsc * dx, gy = gsc * dy, gz = gsc * dz;
+    sgx += gx;
+    sgy += gy;
+    sgz += gz;
+    sq += gx * gx + gy * gy + gz * gz;
+  });
+  const float denom = (sgx * sgx + sgy * sgy + sgz * sgz) + sq;
+  const float f = (cnt < a.min_nb || denom < 1.0e-6f) ? 0.f : 1.0f / denom;
+  a.rho[i] = rho;
+  a.factor[i] = f;
+  a.count[i] = cnt;
+  a.sc2[s] = make_float2(rho, f);
+}
+
+// acceleration_non_pressure (178-226) + predict_velocity (230-242).
+struct AccelArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vs;
+  const float2* sc2;
+  fs_model m;
+  float h, particle_radius, dt;
+  float* accel;
+  float4* vstar;     // cell order (v*, mass)
+};
+
+__global__ void __launch_bounds__(kBlock) k_accel_predict(AccelArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const float4 vi = a.vs[s];
+  const int32_t i = a.g.perm[s];
+  if (!(pf_of(xi) & PF_DYNAMIC)) {
+    st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
+    a.vstar[s] = make_float4(0.f, 0.f, 0.f, vi.w);
+    return;
+  }
+  const float mu = a.m.viscosity[i];
+  const float coh = a.m.surface_tension[i] / vi.w;
+  const float visc_den_add = 0.01f * (a.h * a.h);
+  const CubicK K(a.h);
+  const float h2m = a.h * a.h * 1.000002f;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+    if (t == s) return;
+    const float4 xj = __ldg(a.xs + t);
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r2 = dist2_rn(dx, dy, dz);
+    if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+    const float4 vj = __ldg(a.vs + t);
+    const float rho_j = __ldg(&a.sc2[t].x);
+    const float r = sqrtf(r2);
+    const float wc = coh * vj.w * K.w(fmaxf(r, a.particle_radius));
+    const float vdot = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
+    const float visc = 10.f * mu * (vj.w / fmaxf(rho_j, 1.0e-6f)) * vdot / (r * r + visc_den_add);
+    const float c = visc * K.dw_scale(r) - wc;
+    ax += c * dx;
+    ay += c * dy;
+    az += c * dz;
+  });
+  const float3 g = gravity_of(a.m, i);
+  const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
+  st3(a.accel, i, acc);
+  a.vstar[s] = make_float4(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z, vi.w);
+}
+
+// ---------------------------------------------------- rate + residual ----
+// compute_density_change_rate (246-272), then per mode:
+//   mode 0 (density):    predict_density_star (276-287) and compute_kappa_density (291-306)
+//   mode 1 (divergence): compute_kappa_divergence (357-372)
+// and the residual of _density_residual / _divergence_residual (579-596).
+struct RateArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vstar;      // (v*, mass)
+  const float2* sc2;        // (rho, factor)
+  const float* rest_density;
+  float h, dt, max_kappa, eta;
+  int mode, it;
+  float* d_rho_dt;          // API
+  float* rho_star;          // API (mode 0)
+  float* kappa_new;         // cell order candidate kappa
+  DfsphDev* ctrl;           // null: separate-pass use, no residual
+  double* red_part;
+  int64_t* red_cnt;
+};
+
+__device__ void residual_finish(DfsphDev* ctrl, const double* part, const int64_t* cntp, int nblk, int it,
+                                float eta) {
+  // fixed-order sum over block partials: deterministic
+  __shared__ double sd[kBlock / 32];
+  __shared__ long long sc[kBlock / 32];
+  double v = 0.0;
+  long long c = 0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    v += __ldcg(part + b);
+    c += __ldcg((const long long*)cntp + b);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_down_sync(0xffffffffu, v, o);
+    c += __shfl_down_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sd[threadIdx.x >> 5] = v;
+    sc[threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    long long cn = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      tot += sd[w];
+      cn += sc[w];
+    }
+    const double res = cn > 0 ? tot / (double)cn : 0.0;
+    ctrl->residual = res;
+    ctrl->iters = it + 1;
+    if (it > 0 && res <= (double)eta) ctrl->done = 1;
+    ctrl->ticket = 0;
+  }
+}
+
+__device__ void block_reduce_store(double v, long long c, double* part, int64_t* cntp) {
+  __shared__ double sd[kBlock / 32];
+  __shared__ long long sc[kBlock / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_down_sync(0xffffffffu, v, o);
+    c += __shfl_down_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sd[threadIdx.x >> 5] = v;
+    sc[threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    long long cn = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      tot += sd[w];
+      cn += sc[w];
+    }
+    part[blockIdx.x] = tot;
+    cntp[blockIdx.x] = cn;
+  }
+}
+
+// last-block-done: returns true in exactly one block, after every block's partial is visible
+__device__ bool last_block(uint32_t* ticket) {
+  __shared__ bool am_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (am_last) __threadfence();
+  return am_last;
+}
+
+__global__ void __launch_bounds__(kBlock) k_rate(RateArgs a) {
+  if (a.ctrl && a.ctrl->done) return;  // uniform across the grid: set by an earlier launch
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double term = 0.0;
+  long long dyn = 0;
+  if (s < a.n) {
+    const float4 xi = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    const int pf = pf_of(xi);
+    float d = 0.f;
+    if (pf & PF_ACTIVE) {
+      const float4 vi = a.vstar[s];
+      const CubicK K(a.h);
+      const float h2m = a.h * a.h * 1.000002f;
+      for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+        if (t == s) return;  // zero gradient at r = 0
+        const float4 xj = __ldg(a.xs + t);
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = dist2_rn(dx, dy, dz);
+        if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+        const float4 vj = __ldg(a.vstar + t);
+        const float gs = K.dw_scale(sqrtf(r2));
+        d += vj.w * (gs * ((vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz));
+      });
+    }
+    a.d_rho_dt[i] = d;
+    const float2 rf = a.sc2[s];
+    const bool is_dyn = (pf & PF_DYNAMIC) != 0;
+    float kap = 0.f;
+    if (a.mode == 0) {
+      const float rs = (pf & PF_ACTIVE) ? rf.x + a.dt * d : 0.f;
+      a.rho_star[i] = rs;
+      if (is_dyn) {
+        const float err = fmaxf(rs - a.rest_density[i], 0.f);
+        kap = fminf((err / (a.dt * a.dt)) * rf.y, a.max_kappa);
+        term = (double)err;
+      }
+    } else if (is_dyn) {
+      const float dc = fmaxf(d, 0.f);
+      kap = fminf((1.0f / a.dt) * dc * rf.x * rf.y, a.max_kappa);
+      term = (double)dc;
+    }
+    if (a.kappa_new) a.kappa_new[s] = kap;
+    dyn = is_dyn ? 1 : 0;
+  }
+  if (!a.ctrl) return;
+  block_reduce_store(term, dyn, a.red_part, a.red_cnt);
+  if (last_block(&a.ctrl->ticket)) residual_finish(a.ctrl, a.red_part, a.red_cnt, gridDim.x, a.it, a.eta);
+}
+
+// apply_constant_density_correction (310-337) / apply_divergence_free_correction (376-403)
+struct CorrectArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  float4* vstar;          // in/out (own slot only)
+  const float2* sc2;      // (rho, .)
+  const float* kappa;     // cell order
+  float h, dt;
+  float* kappa_api;       // commit kappa to the API array (may be null)
+  float* vstar_api;       // optional original-order v* output
+  const DfsphDev* ctrl;
+};
+
+__global__ void __launch_bounds__(kBlock) k_correct(CorrectArgs a) {
+  if (a.ctrl && a.ctrl->done) return;
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const int32_t i = a.g.perm[s];
+  const float ki = a.kappa[s];
+  if (a.kappa_api) a.kappa_api[i] = ki;
+  float4 v = a.vstar[s];
+  if (pf_of(xi) & PF_DYNAMIC) {
+    const CubicK K(a.h);
+    const float h2m = a.h * a.h * 1.000002f;
+    const float ci = ki / fmaxf(a.sc2[s].x, 1.0e-6f);
+    float dvx = 0.f, dvy = 0.f, dvz = 0.f;
+    for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+      if (t == s) return;
+      const float4 xj = __ldg(a.xs + t);
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r2 = dist2_rn(dx, dy, dz);
+      if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+      const float coeff = __ldg(&a.vstar[t].w) * (ci + __ldg(a.kappa + t) / fmaxf(__ldg(&a.sc2[t].x), 1.0e-6f));
+      const float c = coeff * K.dw_scale(sqrtf(r2));
+      dvx += c * dx;
+      dvy += c * dy;
+      dvz += c * dz;
+    });
+    v.x = v.x - a.dt * dvx;
+    v.y = v.y - a.dt * dvy;
+    v.z = v.z - a.dt * dvz;
+    a.vstar[s] = v;
+  }
+  if (a.vstar_api) st3(a.vstar_api, i, xyz(v));
+}
+
+// integrate_positions (341-353); also publishes v* in original order.
+__global__ void k_integrate(int64_t n, const int32_t* __restrict__ perm, const float4* __restrict__ xs,
+                            const float4* __restrict__ vstar, float dt, float* x_out, float* vstar_api) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 xi = xs[s];
+  const float4 v = vstar[s];
+  const int32_t i = perm[s];
+  float3 p = xyz(xi);
+  if (pf_of(xi) & PF_DYNAMIC) p = make_float3(xi.x + v.x * dt, xi.y + v.y * dt, xi.z + v.z * dt);
+  st3(x_out, i, p);
+  st3(vstar_api, i, xyz(v));
+}
+
+// copy v* -> particle_qd then apply_bounds (407-442, unconditional damping)
+__global__ void k_final(int64_t n, const int32_t* __restrict__ perm, const float4* __restrict__ xs,
+                        const float4* __restrict__ vstar, Walls walls, float* x_out, float* v_out,
+                        float* vstar_api) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 xi = xs[s];
+  const float4 v4 = vstar[s];
+  const int32_t i = perm[s];
+  float3 p = xyz(xi), v = xyz(v4);
+  st3(vstar_api, i, v);
+  if (pf_of(xi) & PF_DYNAMIC) apply_walls(walls, p, v);
+  st3(x_out, i, p);
+  st3(v_out, i, v);
+}
+
+// mean over dynamic particles of max(a - b, 0): separate-pass residual
+__global__ void k_residual(int64_t n, const int32_t* __restrict__ flags, const int32_t* __restrict__ mask,
+                           const float* __restrict__ av, const float* __restrict__ bv, double* part, int64_t* cntp,
+                           DfsphDev* ctrl, double* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double term = 0.0;
+  long long dyn = 0;
+  if (i < n && (particle_pf(flags, mask, i) & PF_DYNAMIC)) {
+    term = (double)fmaxf(bv ? av[i] - bv[i] : av[i], 0.f);
+    dyn = 1;
+  }
+  block_reduce_store(term, dyn, part, cntp);
+  if (last_block(&ctrl->ticket)) {
+    residual_finish(ctrl, part, cntp, gridDim.x, 0, -1.f);
+    if (threadIdx.x == 0) *out = ctrl->residual;
+  }
+}
+
+int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float dt, float max_kappa, float eta,
+             float* d_rho_dt, float* rho_star, float* kappa_new, DfsphDev* ctrl, cudaStream_t st) {
+  RateArgs a;
+  a.g = grid_view(c);
+  a.n = m->n;
+  a.xs = c->xs;
+  a.vstar = c->vs2;
+  a.sc2 = c->sc2;
+  a.rest_density = m->rest_density;
+  a.h = h;
+  a.dt = dt;
+  a.max_kappa = max_kappa;
+  a.eta = eta;
+  a.mode = mode;
+  a.it = it;
+  a.d_rho_dt = d_rho_dt;
+  a.rho_star = rho_star;
+  a.kappa_new = kappa_new;
+  a.ctrl = ctrl;
+  a.red_part = c->red_part;
+  a.red_cnt = c->red_cnt;
+  k_rate<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  return launch_check("dfsph rate");
+}
+
+int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float* kappa, float* kappa_api,
+                float* vstar_api, const DfsphDev* ctrl, cudaStream_t st) {
+  CorrectArgs a;
+  a.g = grid_view(c);
+  a.n = m->n;
+  a.xs = c->xs;
+  a.vstar = c->vs2;
+  a.sc2 = c->sc2;
+  a.kappa = kappa;
+  a.h = h;
+  a.dt = dt;
+  a.kappa_api = kappa_api;
+  a.vstar_api = vstar_api;
+  a.ctrl = ctrl;
+  k_correct<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  return launch_check("dfsph correct");
+}
+
+int run_density_factor(fs_context* c, const fs_model* m, float h, int min_nb, float* rho, float* factor,
+                       int32_t* count, cudaStream_t st) {
+  DensFactorArgs a;
+  a.g = grid_view(c);
+  a.n = m->n;
+  a.xs = c->xs;
+  a.vs = c->vs2;
+  a.mv = c->mv;
+  a.h = h;
+  a.min_nb = min_nb;
+  a.rho = rho;
+  a.factor = factor;
+  a.count = count;
+  a.sc2 = c->sc2;
+  k_density_factor<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  return launch_check("dfsph density/factor");
+}
+
+}  // namespace
+}  // namespace fs
+
+using namespace fs;
+
+extern "C" {
+
+int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so, const fs_dfsph_params* p,
+                     float* accel, fs_stream_t stream) {
+  if (!c || !m || !si || !so || !p) return set_error(FS_ERR_INVALID, "fs_dfsph_substep: null argument");
+  if (m->n < 0) return set_error(FS_ERR_INVALID, "fs_dfsph_substep: negative n");
+  if (m->n == 0) return FS_OK;
+  if (!m->particle_flags || !m->particle_mask || !m->particle_mass || !m->gravity || m->n_worlds < 1 ||
+      !m->rest_density || !m->viscosity || !m->surface_tension || !si->particle_q || !si->particle_qd ||
+      !so->particle_q || !so->particle_qd || !so->rho || !so->factor || !so->rho_star || !so->d_rho_dt ||
+      !so->kappa || !so->kappa_v || !so->neighbor_count || !so->v_star || !accel)
+    return set_error(FS_ERR_INVALID, "fs_dfsph_substep: missing array");
+  if (p->warm_start && (!si->kappa || !si->kappa_v))
+    return set_error(FS_ERR_INVALID, "fs_dfsph_substep: warm_start needs state_in kappa/kappa_v");
+  if (m->n > c->capacity) return set_error(FS_ERR_CAPACITY, "fs_dfsph_substep: n > capacity");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n = m->n;
+  const float h = p->smoothing_length, dt = p->dt;
+  int rc;
+  if ((rc = check_cuda(cudaMemsetAsync(c->dfsph, 0, sizeof(DfsphDev) * 2, st), "dfsph reset"))) return rc;
+  // ---- first half: positions x_in
+  if ((rc = grid_build(c, si->particle_q, n, h, st))) return rc;
+  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, si->particle_q, si->particle_qd, c->xs, c->vs,
+                                                    c->mv, c->status);
+  {
+    // density/factor reads masses from vs2.w: fill it from vs (v_in, mass) first
+    if ((rc = check_cuda(cudaMemcpyAsync(c->vs2, c->vs, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st),
+                         "dfsph copy")))
+      return rc;
+  }
+  if ((rc = run_density_factor(c, m, h, p->min_neighbors_for_factor, so->rho, so->factor, so->neighbor_count, st)))
+    return rc;
+  AccelArgs aa;
+  aa.g = grid_view(c);
+  aa.n = n;
+  aa.xs = c->xs;
+  aa.vs = c->vs;
+  aa.sc2 = c->sc2;
+  aa.m = *m;
+  aa.h = h;
+  aa.particle_radius = p->particle_radius;
+  aa.dt = dt;
+  aa.accel = accel;
+  aa.vstar = c->vs2;
+  k_accel_predict<<<blocks_for(n), kBlock, 0, st>>>(aa);
+  if ((rc = launch_check("dfsph accel"))) return rc;
+  if (p->warm_start) {
+    k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa, c->sc1, nullptr);
+    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa, nullptr, nullptr, st))) return rc;
+  }
+  for (int it = 0; it < p->max_rho_iterations; ++it) {
+    if ((rc = run_rate(c, m, 0, it, h, dt, p->max_kappa, p->eta_density, so->d_rho_dt, so->rho_star, c->sc1,
+                       c->dfsph + 0, st)))
+      return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa, nullptr, c->dfsph + 0, st))) return rc;
+  }
+  k_integrate<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, dt, so->particle_q, so->v_star);
+  if ((rc = launch_check("dfsph integrate"))) return rc;
+  // ---- second half: positions x_out
+  if ((rc = grid_build(c, so->particle_q, n, h, st))) return rc;
+  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, so->particle_q, so->v_star, c->xs, c->vs2, c->mv,
+                                                    c->status);
+  if ((rc = run_density_factor(c, m, h, p->min_neighbors_for_factor, so->rho, so->factor, so->neighbor_count, st)))
+    return rc;
+  if (p->warm_start) {
+    k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa_v, c->sc1, nullptr);
+    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa_v, nullptr, nullptr, st))) return rc;
+  }
+  for (int it = 0; it < p->max_vel_iterations; ++it) {
+    if ((rc = run_rate(c, m, 1, it, h, dt, p->max_kappa_v, p->eta_divergence, so->d_rho_dt, nullptr, c->sc1,
+                       c->dfsph + 1, st)))
+      return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa_v, nullptr, c->dfsph + 1, st))) return rc;
+  }
+  const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 1, 0.f, 0.f);
+  k_final<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, w, so->particle_q, so->particle_qd, so->v_star);
+  c->last_stream = st;
+  return launch_check("dfsph final");
+}
+
+int fs_dfsph_info_read(fs_context* c, fs_dfsph_info* info) {
+  if (!c || !info) return set_error(FS_ERR_INVALID, "fs_dfsph_info_read: bad arguments");
+  DeviceGuard dg(c->device);
+  DfsphDev h[2];
+  int rc = check_cuda(cudaMemcpyAsync(h, c->dfsph, sizeof(h), cudaMemcpyDeviceToHost, c->last_stream),
+                      "fs_dfsph_info_read");
+  if (!rc) rc = check_cuda(cudaStreamSynchronize(c->last_stream), "fs_dfsph_info_read: sync");
+  if (rc) return rc;
+  info->rho_iterations = h[0].iters;
+  info->vel_iterations = h[1].iters;
+  info->density_residual = h[0].residual;
+  info->divergence_residual = h[1].residual;
+  return FS_OK;
+}
+
+int fs_dfsph_density_factor(fs_context* c, const fs_model* m, const float* x, float h, int32_t min_nb, float* rho,
+                            float* factor, int32_t* neighbor_count, fs_stream_t stream) {
+  if (!c || !m || !x || !rho || !factor || !neighbor_count)
+    return set_error(FS_ERR_INVALID, "fs_dfsph_density_factor: null argument");
+  if (m->n == 0) return FS_OK;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_dfsph_density_factor: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, x, c->xs, c->vs2, c->mv, c->status);
+  return run_density_factor(c, m, h, min_nb, rho, factor, neighbor_count, st);
+}
+
+int fs_dfsph_divergence(fs_context* c, const fs_model* m, const float* x, const float* v, float h, float* d_rho_dt,
+                        fs_stream_t stream) {
+  if (!c || !m || !x || !v || !d_rho_dt) return set_error(FS_ERR_INVALID, "fs_dfsph_divergence: null argument");
+  if (m->n == 0) return FS_OK;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_dfsph_divergence: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, v, c->xs, c->vs2, nullptr, c->status);
+  // rho/factor are not needed for the rate itself (mode 1 reads them only for kappa, which is discarded)
+  if (cudaMemsetAsync(c->sc2, 0, sizeof(float2) * m->n, st) != cudaSuccess)
+    return set_error(FS_ERR_CUDA, "fs_dfsph_divergence: memset");
+  return run_rate(c, m, 1, 0, h, 1.f, 0.f, 0.f, d_rho_dt, nullptr, nullptr, nullptr, st);
+}
+
+int fs_dfsph_correct(fs_context* c, const fs_model* m, const float* x, float* v_star, const float* rho,
+                     const float* kappa, float h, float dt, fs_stream_t stream) {
+  if (!c || !m || !x || !v_star || !rho || !kappa) return set_error(FS_ERR_INVALID, "fs_dfsph_correct: null argument");
+  if (m->n == 0) return FS_OK;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_dfsph_correct: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, v_star, c->xs, c->vs2, nullptr,
+                                                       c->status);
+  k_gather_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, rho, nullptr, c->sc2);
+  k_gather_scalar<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, kappa, c->sc1, nullptr);
+  return run_correct(c, m, h, dt, c->sc1, nullptr, v_star, nullptr, st);
+}
+
+int fs_dfsph_residual(fs_context* c, const fs_model* m, const float* a, const float* b, double* out,
+                      fs_stream_t stream) {
+  if (!c || !m || !a || !out || !m->particle_flags) return set_error(FS_ERR_INVALID, "fs_dfsph_residual: bad args");
+  if (m->n > c->capacity) return set_error(FS_ERR_CAPACITY, "fs_dfsph_residual: n > capacity");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n = m->n > 0 ? m->n : 1;
+  if (cudaMemsetAsync(c->dfsph, 0, sizeof(DfsphDev), st) != cudaSuccess)
+    return set_error(FS_ERR_CUDA, "fs_dfsph_residual: memset");
+  k_residual<<<blocks_for(n), kBlock, 0, st>>>(m->n, m->particle_flags, m->particle_mask, a, b, c->red_part,
+                                               c->red_cnt, c->dfsph, out);
+  return launch_check("fs_dfsph_residual");
+}
+
+}  // extern "C"

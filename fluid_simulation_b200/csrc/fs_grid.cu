@@ -1,0 +1,370 @@
+// Hash-grid build: the B200 replacement of warp's wp.HashGrid.build
+// (called at solver_wcsph.py:456, solver_dfsph.py:624/783, solver_pbf.py:737/858).
+//
+// Result (identical to a stable radix sort of (cell key, particle id)):
+//   perm[s]      original index of the particle in sorted slot s
+//   off[c]       first slot of cell c; off[c+1] one past its last slot
+// Algorithm (O(N) + O(cells) HBM traffic, deterministic):
+//   1. keys:    cell key per particle, arrival slot by atomicAdd on the cell count
+//   2. scan:    exclusive prefix of the counts (three-phase block scan)
+//   3. scatter: tmp[off[key] + arrival] = i        (order inside a cell arbitrary)
+//   4. rank:    slot = off[key] + #{j in cell : j < i}; perm[slot] = i
+// Step 4 restores ascending original index inside each cell, which is the
+// order warp's stable radix sort produces, so results do not depend on the
+// order in which atomics were served.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "fs_internal.cuh"
+
+namespace fs {
+
+namespace {
+
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 4096 cells per block
+
+__global__ void k_cell_keys(int64_t n, const float* __restrict__ x, float inv, int dim_x, int dim_y, int dim_z,
+                            int rounding, int32_t* __restrict__ key, int32_t* __restrict__ slot,
+                            int32_t* __restrict__ count, uint32_t* status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
+  if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(status, FS_STATUS_NONFINITE);
+  GridDev g;
+  g.dim_x = dim_x;
+  g.dim_y = dim_y;
+  g.dim_z = dim_z;
+  const int k = phys_cell(g, to_cell(__fmul_rn(px, inv), rounding), to_cell(__fmul_rn(py, inv), rounding),
+                          to_cell(__fmul_rn(pz, inv), rounding));
+  key[i] = k;
+  slot[i] = atomicAdd(count + k, 1);
+}
+
+// phase 1: per-tile sums
+__global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t m, int32_t* __restrict__ part) {
+  __shared__ int32_t warp_sums[kScanThreads / 32];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int64_t j = base + k;
+    if (j < m) s += in[j];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int32_t v = threadIdx.x < kScanThreads / 32 ? warp_sums[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+  }
+}
+
+// block-wide exclusive scan of one value per thread (blockDim multiple of 32, <= 1024)
+__device__ int32_t block_exclusive_scan(int32_t v, int32_t* total) {
+  __shared__ int32_t ws[32];
+  __shared__ int32_t block_total;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  int32_t inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) ws[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    int32_t w = lane < nw ? ws[lane] : 0;
+    int32_t wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    if (lane < nw) ws[lane] = wi - w;  // exclusive prefix of warp sums
+    if (lane == nw - 1) block_total = wi;
+  }
+  __syncthreads();
+  const int32_t res = inc - v + ws[wid];
+  if (total) *total = block_total;
+  __syncthreads();
+  return res;
+}
+
+// phase 2: exclusive scan of the tile sums (one block, <= 1024 * 4 tiles)
+__global__ void k_scan_partials(int32_t* part, int nb) {
+  constexpr int kItems = 4;
+  const int base = threadIdx.x * kItems;
+  int32_t v[kItems];
+  int32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    v[k] = base + k < nb ? part[base + k] : 0;
+    s += v[k];
+  }
+  int32_t total = 0;
+  int32_t run = block_exclusive_scan(s, &total);
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    if (base + k < nb) part[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0) part[nb] = total;
+}
+
+// phase 3: scan inside tiles, offset by the tile prefix; out has m + 1 entries
+__global__ void k_scan_down(const int32_t* __restrict__ in, int64_t m, const int32_t* __restrict__ part,
+                            int32_t* __restrict__ out) {
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int32_t v[kScanItems];
+  int32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int64_t j = base + k;
+    v[k] = j < m ? in[j] : 0;
+    s += v[k];
+  }
+  int32_t run = block_exclusive_scan(s, nullptr) + part[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int64_t j = base + k;
+    if (j < m) out[j] = run;
+    run += v[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[m] = part[gridDim.x];
+}
+
+__global__ void k_scatter(int64_t n, const int32_t* __restrict__ key, const int32_t* __restrict__ slot,
+                          const int32_t* __restrict__ off, int32_t* __restrict__ tmp) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  tmp[off[key[i]] + slot[i]] = (int32_t)i;
+}
+
+__global__ void k_rank(int64_t n, const int32_t* __restrict__ key, const int32_t* __restrict__ off,
+                       const int32_t* __restrict__ tmp, int32_t* __restrict__ perm) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int32_t i = tmp[s];
+  const int32_t c = key[i];
+  const int32_t a = off[c], b = off[c + 1];
+  int32_t rank = 0;
+  for (int32_t t = a; t < b; ++t) rank += tmp[t] < i ? 1 : 0;
+  perm[a + rank] = i;
+}
+
+__global__ void k_tables(int64_t n, int64_t ncell, const int32_t* __restrict__ perm, const int32_t* __restrict__ key,
+                         const int32_t* __restrict__ off, int32_t* point_ids, int32_t* point_cells,
+                         int32_t* cell_starts, int32_t* cell_ends) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) {
+    const int32_t i = perm[t];
+    if (point_ids) point_ids[t] = i;
+    if (point_cells) point_cells[t] = key[i];
+  }
+  if (t < ncell) {
+    if (cell_starts) cell_starts[t] = off[t];
+    if (cell_ends) cell_ends[t] = off[t + 1];
+  }
+}
+
+template <bool FILL>
+__global__ void k_candidates(GridDev g, const float* __restrict__ q, int64_t nq, float r, int64_t* counts,
+                             const int64_t* __restrict__ offsets, int32_t* cand) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  int64_t k = 0;
+  const int64_t base = FILL ? offsets[i] : 0;
+  for_each_candidate(g, q[3 * i], q[3 * i + 1], q[3 * i + 2], r, [&](int t) {
+    if (FILL) cand[base + k] = g.perm[t];
+    ++k;
+  });
+  counts[i] = k;
+}
+
+}  // namespace
+
+int scan_blocks(int64_t m) { return (int)((m + kScanTile - 1) / kScanTile); }
+
+GridDev grid_view(const fs_context* c) {
+  GridDev g;
+  g.off = c->cell_off;
+  g.perm = c->perm;
+  g.dim_x = c->grid.dim_x;
+  g.dim_y = c->grid.dim_y;
+  g.dim_z = c->grid.dim_z;
+  g.rounding = c->grid.rounding;
+  g.inv = c->built_inv;
+  return g;
+}
+
+int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st) {
+  if (n < 0 || (n > 0 && !x) || !(radius > 0.f)) return set_error(FS_ERR_INVALID, "grid_build: bad arguments");
+  if (n > c->capacity) return set_error(FS_ERR_CAPACITY, "grid_build: n=%lld > capacity=%lld", (long long)n,
+                                        (long long)c->capacity);
+  const float inv = 1.0f / radius;
+  int rc = check_cuda(cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * c->ncell, st), "memset cell counts");
+  if (rc) return rc;
+  if (n > 0)
+    k_cell_keys<<<blocks_for(n), kBlock, 0, st>>>(n, x, inv, c->grid.dim_x, c->grid.dim_y, c->grid.dim_z,
+                                                   c->grid.rounding, c->key, c->slot, c->cell_count, c->status);
+  const int nb = scan_blocks(c->ncell);
+  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part);
+  k_scan_partials<<<1, 1024, 0, st>>>(c->scan_part, nb);
+  k_scan_down<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, c->cell_off);
+  if (n > 0) {
+    k_scatter<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->slot, c->cell_off, c->tmp_ids);
+    k_rank<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->cell_off, c->tmp_ids, c->perm);
+  }
+  rc = launch_check("grid_build");
+  if (rc) return rc;
+  c->built_n = n;
+  c->built_inv = inv;
+  c->last_stream = st;
+  return FS_OK;
+}
+
+}  // namespace fs
+
+using namespace fs;
+
+// ------------------------------------------------------------ error state --
+namespace fs {
+static thread_local char g_err[512] = "";
+
+int set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return FS_OK;
+  return set_error(FS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int launch_check(const char* what) { return check_cuda(cudaGetLastError(), what); }
+}  // namespace fs
+
+extern "C" {
+
+const char* fs_last_error_string(void) { return fs::g_err; }
+const char* fs_version(void) { return "fluid_b200 0.1 (sm_100a)"; }
+
+int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* grid, int32_t device) {
+  if (!out || capacity < 0 || !grid || grid->dim_x <= 0 || grid->dim_y <= 0 || grid->dim_z <= 0 ||
+      (grid->rounding != 0 && grid->rounding != 1))
+    return set_error(FS_ERR_INVALID, "fs_context_create: bad arguments");
+  const int64_t ncell = (int64_t)grid->dim_x * grid->dim_y * grid->dim_z;
+  if (ncell > (int64_t)kScanTile * 4096 || capacity > (int64_t)0x7fffffff)
+    return set_error(FS_ERR_INVALID, "fs_context_create: grid of %lld cells or capacity too large",
+                     (long long)ncell);
+  DeviceGuard dg(device);
+  fs_context* c = new fs_context();
+  c->device = device;
+  c->capacity = capacity;
+  c->grid = *grid;
+  c->ncell = ncell;
+  const int64_t cap = capacity > 0 ? capacity : 1;
+  const int nb = scan_blocks(ncell);
+  const int rb = reduction_blocks(cap);
+  struct A {
+    void** p;
+    size_t bytes;
+  } allocs[] = {
+      {(void**)&c->key, sizeof(int32_t) * cap},         {(void**)&c->slot, sizeof(int32_t) * cap},
+      {(void**)&c->cell_count, sizeof(int32_t) * ncell}, {(void**)&c->cell_off, sizeof(int32_t) * (ncell + 1)},
+      {(void**)&c->tmp_ids, sizeof(int32_t) * cap},     {(void**)&c->perm, sizeof(int32_t) * cap},
+      {(void**)&c->scan_part, sizeof(int32_t) * (nb + 1)},
+      {(void**)&c->xs, sizeof(float4) * cap},           {(void**)&c->xs2, sizeof(float4) * cap},
+      {(void**)&c->vs, sizeof(float4) * cap},           {(void**)&c->vs2, sizeof(float4) * cap},
+      {(void**)&c->mv, sizeof(float) * cap},            {(void**)&c->sc2, sizeof(float2) * cap},
+      {(void**)&c->sc1, sizeof(float) * cap},           {(void**)&c->sc1b, sizeof(float) * cap},
+      {(void**)&c->xo_tmp, sizeof(float) * 3 * cap},    {(void**)&c->vo_tmp, sizeof(float) * 3 * cap},
+      {(void**)&c->red_part, sizeof(double) * rb},      {(void**)&c->red_cnt, sizeof(int64_t) * rb},
+      {(void**)&c->dfsph, sizeof(DfsphDev) * 2},         {(void**)&c->status, sizeof(uint32_t)},
+  };
+  for (auto& a : allocs) {
+    cudaError_t e = cudaMalloc(a.p, a.bytes);
+    if (e != cudaSuccess) {
+      int rc = check_cuda(e, "fs_context_create: cudaMalloc");
+      fs_context_destroy(c);
+      return rc;
+    }
+  }
+  int rc = check_cuda(cudaMemset(c->status, 0, sizeof(uint32_t)), "fs_context_create: memset");
+  if (!rc) rc = check_cuda(cudaMemset(c->dfsph, 0, sizeof(DfsphDev) * 2), "fs_context_create: memset");
+  if (rc) {
+    fs_context_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return FS_OK;
+}
+
+int fs_context_destroy(fs_context* c) {
+  if (!c) return FS_OK;
+  DeviceGuard dg(c->device);
+  void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->scan_part, c->xs, c->xs2,
+                c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
+                c->dfsph, c->status};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  delete c;
+  return FS_OK;
+}
+
+int64_t fs_context_capacity(const fs_context* c) { return c ? c->capacity : -1; }
+
+int fs_grid_build(fs_context* c, const float* x, int64_t n, float radius, fs_stream_t stream) {
+  if (!c) return set_error(FS_ERR_INVALID, "fs_grid_build: null context");
+  DeviceGuard dg(c->device);
+  return grid_build(c, x, n, radius, (cudaStream_t)stream);
+}
+
+int fs_grid_tables(fs_context* c, int32_t* point_ids, int32_t* point_cells, int32_t* cell_starts,
+                   int32_t* cell_ends, fs_stream_t stream) {
+  if (!c) return set_error(FS_ERR_INVALID, "fs_grid_tables: null context");
+  if (c->built_n < 0) return set_error(FS_ERR_NOGRID, "fs_grid_tables: no grid built");
+  DeviceGuard dg(c->device);
+  const int64_t m = c->built_n > c->ncell ? c->built_n : c->ncell;
+  k_tables<<<blocks_for(m), kBlock, 0, (cudaStream_t)stream>>>(c->built_n, c->ncell, c->perm, c->key, c->cell_off,
+                                                               point_ids, point_cells, cell_starts, cell_ends);
+  return launch_check("fs_grid_tables");
+}
+
+int fs_grid_candidates(fs_context* c, const float* q, int64_t nq, float r, int64_t* counts, const int64_t* offsets,
+                       int32_t* cand, fs_stream_t stream) {
+  if (!c || nq < 0 || (nq > 0 && (!q || !counts)) || (cand && !offsets))
+    return set_error(FS_ERR_INVALID, "fs_grid_candidates: bad arguments");
+  if (c->built_n < 0) return set_error(FS_ERR_NOGRID, "fs_grid_candidates: no grid built");
+  if (nq == 0) return FS_OK;
+  DeviceGuard dg(c->device);
+  GridDev g = grid_view(c);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cand)
+    k_candidates<true><<<blocks_for(nq), kBlock, 0, st>>>(g, q, nq, r, counts, offsets, cand);
+  else
+    k_candidates<false><<<blocks_for(nq), kBlock, 0, st>>>(g, q, nq, r, counts, nullptr, nullptr);
+  return launch_check("fs_grid_candidates");
+}
+
+int fs_status_read(fs_context* c, uint32_t* status) {
+  if (!c || !status) return set_error(FS_ERR_INVALID, "fs_status_read: bad arguments");
+  DeviceGuard dg(c->device);
+  int rc = check_cuda(cudaMemcpyAsync(status, c->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->last_stream),
+                      "fs_status_read");
+  if (rc) return rc;
+  return check_cuda(cudaStreamSynchronize(c->last_stream), "fs_status_read: sync");
+}
+
+int fs_status_clear(fs_context* c, fs_stream_t stream) {
+  if (!c) return set_error(FS_ERR_INVALID, "fs_status_clear: null context");
+  DeviceGuard dg(c->device);
+  return check_cuda(cudaMemsetAsync(c->status, 0, sizeof(uint32_t), (cudaStream_t)stream), "fs_status_clear");
+}
+
+}  // extern "C"

@@ -1,0 +1,313 @@
+// Internal declarations shared by the CUDA translation units of libfluid_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fluid_b200.h"
+
+// ------------------------------------------------------------------ layout --
+// Cell-sorted particle data lives in the context (HBM), one slot per particle
+// in hash-cell order, so every neighbour loop reads contiguous slot ranges:
+//   xs[s]  float4 (x, y, z, packed flags)        -- position stream
+//   vs[s]  float4 (vx, vy, vz, mass)              -- velocity stream
+//   mv[s]  float   rest_density * volume          -- density weight
+// Packed flags (bits of the .w word): PF_ACTIVE = ParticleFlags.ACTIVE,
+// PF_DYNAMIC = active && particle_mask == 0.
+namespace fs {
+
+constexpr int PF_ACTIVE = 1;
+constexpr int PF_DYNAMIC = 2;
+constexpr int kBlock = 256;
+
+struct DfsphDev {     // device-resident per-step DFSPH control block
+  int32_t done;       // residual test passed: later kernels of this half exit
+  int32_t iters;      // iterations entered in this half
+  uint32_t ticket;    // last-block-done counter of the residual reduction
+  int32_t pad;
+  double residual;    // last residual of this half
+};
+
+struct GridDev {
+  const int32_t* off;   // [ncell + 1] exclusive prefix of cell occupancy (hash-key order)
+  const int32_t* perm;  // [n] sorted slot -> original particle index (warp's point_ids)
+  int32_t dim_x, dim_y, dim_z, rounding;
+  float inv;            // 1 / cell width, float32 as warp
+};
+
+}  // namespace fs
+
+struct fs_context {
+  int32_t device = 0;
+  int64_t capacity = 0;
+  fs_grid_config grid{};
+  int64_t ncell = 0;
+  int64_t built_n = -1;      // n of the last grid build, -1 = none
+  float built_inv = 0.f;
+  cudaStream_t last_stream = nullptr;
+
+  // grid build
+  int32_t* key = nullptr;        // [cap] cell key of original particle i
+  int32_t* slot = nullptr;       // [cap] arrival slot inside the cell
+  int32_t* cell_count = nullptr; // [ncell]
+  int32_t* cell_off = nullptr;   // [ncell + 1]
+  int32_t* tmp_ids = nullptr;    // [cap] unordered-in-cell ids
+  int32_t* perm = nullptr;       // [cap] sorted slot -> original index
+  int32_t* scan_part = nullptr;  // [scan blocks + 1]
+
+  // cell-sorted streams
+  float4* xs = nullptr;   // positions + packed flags
+  float4* xs2 = nullptr;  // second position buffer (PBF Jacobi double buffer)
+  float4* vs = nullptr;   // velocities + mass
+  float4* vs2 = nullptr;  // second velocity buffer (DFSPH v*, PBF x_in)
+  float* mv = nullptr;    // rest_density * volume
+  float2* sc2 = nullptr;  // per-slot scalar pair (rho, p) / (rho, factor)
+  float* sc1 = nullptr;   // per-slot scalar (kappa / lambda)
+  float* sc1b = nullptr;  // per-slot scalar (second)
+  float* xo_tmp = nullptr;  // [cap*3] original-order scratch positions (PBF x_pred)
+  float* vo_tmp = nullptr;  // [cap*3] original-order scratch velocities (PBF v_pred)
+
+  // reductions / status
+  double* red_part = nullptr;   // [reduction blocks]
+  int64_t* red_cnt = nullptr;   // [reduction blocks]
+  fs::DfsphDev* dfsph = nullptr; // [2] control blocks (density half, divergence half)
+  uint32_t* status = nullptr;
+};
+
+namespace fs {
+
+// --------------------------------------------------------------- host util --
+int set_error(int code, const char* fmt, ...);
+int check_cuda(cudaError_t e, const char* what);
+int launch_check(const char* what);
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+inline int blocks_for(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+// grid build (fs_grid.cu)
+int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st);
+GridDev grid_view(const fs_context* c);
+
+// DFSPH residual helper shared with the separate-pass entry (fs_dfsph.cu)
+int reduction_blocks(int64_t n);
+
+// ----------------------------------------------------------- device math --
+#define FS_DEV __device__ __forceinline__
+
+constexpr float kPi = 3.14159265358979323846f;
+
+FS_DEV int pf_of(float4 p) { return __float_as_int(p.w); }
+FS_DEV float pack_pf(int pf) { return __int_as_float(pf); }
+
+// Distance computed with individually rounded operations (no FMA), so that
+// decisions such as `r < h` are bit-identical to a strict FP32 evaluation.
+FS_DEV float dist2_rn(float dx, float dy, float dz) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+struct CubicK {   // constants of the cubic spline of support h
+  float h, k;     // k = 8 / (pi h^3)
+  FS_DEV explicit CubicK(float h_) : h(h_), k(8.0f / (kPi * (h_ * h_ * h_))) {}
+  // W(r), solver_wcsph.py:21-34
+  FS_DEV float w(float r) const {
+    const float q = r / h;
+    float res = 0.f;
+    if (q <= 1.f) {
+      if (q <= 0.5f) {
+        const float q2 = q * q;
+        const float q3 = q2 * q;
+        res = k * (6.f * q3 - 6.f * q2 + 1.f);
+      } else {
+        const float t = 1.f - q;
+        res = 2.f * k * (t * t * t);
+      }
+    }
+    return res;
+  }
+  // scalar s with grad W(d) = s * d for |d| = r, solver_wcsph.py:37-51
+  FS_DEV float dw_scale(float r) const {
+    const float q = r / h;
+    float s = 0.f;
+    if (r > 1.0e-5f && q <= 1.f) {
+      const float inv = 1.f / (r * h);
+      if (q <= 0.5f) {
+        s = 6.f * k * q * (3.f * q - 2.f) * inv;
+      } else {
+        const float t = 1.f - q;
+        s = -6.f * k * t * t * inv;
+      }
+    }
+    return s;
+  }
+};
+
+struct PbfK {     // poly6 / spiky constants, solver_pbf.py:24-45
+  float h, h2, kw, kg;
+  FS_DEV explicit PbfK(float h_) : h(h_), h2(h_ * h_) {
+    const float c = h_ * h_ * h_;
+    kw = 315.0f / (64.0f * kPi * (c * c * c));
+    kg = -45.0f / (kPi * (c * c));
+  }
+  FS_DEV float w(float r) const {
+    float res = 0.f;
+    if (h > 0.f && r < h) {
+      const float rhs = h2 - r * r;
+      res = kw * (rhs * rhs * rhs);
+    }
+    return res;
+  }
+  FS_DEV float dw_scale(float r) const {  // spiky gradient = s * d
+    float s = 0.f;
+    if (h > 0.f && r > 1.0e-6f && r < h) s = kg * ((h - r) * (h - r) / r);
+    return s;
+  }
+};
+
+// ------------------------------------------------------ neighbour queries --
+FS_DEV int to_cell(float v, int rounding) {
+  if (!(v == v)) return 0;
+  if (rounding == 1) v = floorf(v);
+  if (v > 536870912.0f) return 536870912;
+  if (v < -536870912.0f) return -536870912;
+  return __float2int_rz(v);
+}
+
+FS_DEV int wrap_axis(int v, int dim) {
+  v += (1 << 20);
+  v = v < 0 ? 0 : v;
+  return v % dim;
+}
+
+FS_DEV int phys_cell(const GridDev& g, int x, int y, int z) {
+  return (wrap_axis(z, g.dim_z) * g.dim_y + wrap_axis(y, g.dim_y)) * g.dim_x + wrap_axis(x, g.dim_x);
+}
+
+// Visits the candidates of warp's hash_grid_query(grid, p, r) in the same
+// order: cells z-outer, y-middle, x-inner, each cell's slots in sorted order.
+// f(t) receives the cell-sorted SLOT t (original index = perm[t]).  A run of
+// consecutive x cells is one contiguous slot range because cell offsets are a
+// prefix sum in hash-key order; a run that wraps modulo dim_x splits in two.
+template <class F>
+FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f) {
+  const int x0 = to_cell(__fmul_rn(__fsub_rn(px, r), g.inv), g.rounding);
+  const int y0 = to_cell(__fmul_rn(__fsub_rn(py, r), g.inv), g.rounding);
+  const int z0 = to_cell(__fmul_rn(__fsub_rn(pz, r), g.inv), g.rounding);
+  const int x1 = min(to_cell(__fmul_rn(__fadd_rn(px, r), g.inv), g.rounding), x0 + g.dim_x - 1);
+  const int y1 = min(to_cell(__fmul_rn(__fadd_rn(py, r), g.inv), g.rounding), y0 + g.dim_y - 1);
+  const int z1 = min(to_cell(__fmul_rn(__fadd_rn(pz, r), g.inv), g.rounding), z0 + g.dim_z - 1);
+  const int nx = x1 - x0 + 1;
+  const int xa = x0 + (1 << 20);
+  for (int z = z0; z <= z1; ++z) {
+    const int cz = wrap_axis(z, g.dim_z);
+    for (int y = y0; y <= y1; ++y) {
+      const int row = (cz * g.dim_y + wrap_axis(y, g.dim_y)) * g.dim_x;
+      if (xa >= 0) {
+        const int cx0 = xa % g.dim_x;
+        const int len1 = min(nx, g.dim_x - cx0);
+        int s = __ldg(g.off + row + cx0);
+        int e = __ldg(g.off + row + cx0 + len1);
+        for (int t = s; t < e; ++t) f(t);
+        if (nx > len1) {
+          s = __ldg(g.off + row);
+          e = __ldg(g.off + row + (nx - len1));
+          for (int t = s; t < e; ++t) f(t);
+        }
+      } else {  // far outside the shifted range: cells clamp, visit one by one
+        for (int x = x0; x <= x1; ++x) {
+          const int c = row + wrap_axis(x, g.dim_x);
+          const int e = __ldg(g.off + c + 1);
+          for (int t = __ldg(g.off + c); t < e; ++t) f(t);
+        }
+      }
+    }
+  }
+}
+
+// Box walls of the reference's apply_bounds variants.
+//   mode 0: WCSPH  (solver_wcsph.py:264-305) clamp to [-W,W]x[-H,H]x[0,2L], damp outward v
+//   mode 1: DFSPH  (solver_dfsph.py:407-442) same walls, damping unconditional
+//   mode 2: PBF    (solver_pbf.py:467-517)  walls inset by radius + eps, damp outward v
+struct Walls {
+  float xmin, xmax, ymin, ymax, zmin, zmax, damping;
+  int mode;
+};
+
+inline Walls make_walls(float w, float hgt, float l, float damping, int mode, float radius, float eps) {
+  Walls b;
+  b.mode = mode;
+  b.damping = damping;
+  if (mode == 2) {
+    b.xmin = -w + radius + eps;
+    b.xmax = w - radius - eps;
+    b.ymin = -hgt + radius + eps;
+    b.ymax = hgt - radius - eps;
+    b.zmin = radius + eps;
+    b.zmax = l * 2.0f - radius - eps;
+  } else {
+    b.xmin = -w;
+    b.xmax = w;
+    b.ymin = -hgt;
+    b.ymax = hgt;
+    b.zmin = 0.f;
+    b.zmax = l * 2.0f;
+  }
+  return b;
+}
+
+FS_DEV void apply_walls(const Walls& b, float3& p, float3& v) {
+  const bool cond = b.mode != 1;
+  if (p.x < b.xmin) { p.x = b.xmin; if (!cond || v.x < 0.f) v.x = v.x * b.damping; }
+  if (p.x > b.xmax) { p.x = b.xmax; if (!cond || v.x > 0.f) v.x = v.x * b.damping; }
+  if (p.y < b.ymin) { p.y = b.ymin; if (!cond || v.y < 0.f) v.y = v.y * b.damping; }
+  if (p.y > b.ymax) { p.y = b.ymax; if (!cond || v.y > 0.f) v.y = v.y * b.damping; }
+  if (p.z < b.zmin) { p.z = b.zmin; if (!cond || v.z < 0.f) v.z = v.z * b.damping; }
+  if (p.z > b.zmax) { p.z = b.zmax; if (!cond || v.z > 0.f) v.z = v.z * b.damping; }
+}
+
+// apply_position_bounds, solver_pbf.py:367-399 (walls of mode 2, no velocity)
+FS_DEV void clamp_position(const Walls& b, float3& p) {
+  if (p.x < b.xmin) p.x = b.xmin;
+  if (p.x > b.xmax) p.x = b.xmax;
+  if (p.y < b.ymin) p.y = b.ymin;
+  if (p.y > b.ymax) p.y = b.ymax;
+  if (p.z < b.zmin) p.z = b.zmin;
+  if (p.z > b.zmax) p.z = b.zmax;
+}
+
+FS_DEV float3 ld3(const float* p, int64_t i) { return make_float3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+FS_DEV void st3(float* p, int64_t i, float3 v) {
+  p[3 * i] = v.x;
+  p[3 * i + 1] = v.y;
+  p[3 * i + 2] = v.z;
+}
+FS_DEV float3 xyz(float4 a) { return make_float3(a.x, a.y, a.z); }
+
+FS_DEV int particle_pf(const int32_t* flags, const int32_t* mask, int64_t i) {
+  const bool act = (flags[i] & 1) != 0;
+  const bool dyn = act && (mask ? mask[i] == 0 : true);
+  return (act ? PF_ACTIVE : 0) | (dyn ? PF_DYNAMIC : 0);
+}
+
+FS_DEV float3 gravity_of(const fs_model& m, int64_t i) {
+  // reference: gravity[max(world, 0)]; an index past the last world (which
+  // the reference would read out of bounds) is clamped here and reported as
+  // FS_STATUS_BOUNDS by the gather.
+  int w = m.particle_world ? m.particle_world[i] : 0;
+  w = w < 0 ? 0 : w;
+  w = w >= m.n_worlds ? m.n_worlds - 1 : w;
+  return ld3(m.gravity, w);
+}
+
+}  // namespace fs

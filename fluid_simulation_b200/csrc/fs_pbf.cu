@@ -1,0 +1,561 @@
+// PBF substep on B200 (replaces SolverPBF.step, solver_pbf.py:676-954).
+//
+//   predict   v_pred = v + dt g; x_pred = x + dt v_pred; position bounds  (original order)
+//   grid build(x_pred)          -- the only build unless rebuild_grid_each_iteration
+//   gather    x_pred, v_pred, x_in, mass, flags -> cell order
+//   density   (poly6)
+//   accel     non-pressure (PBF variant) + apply_non_pressure_prediction + bounds -> x_pred'
+//   repeat max_iterations:
+//     lambda  rho, C, lambda, neighbour count
+//     delta   dx (+ s_corr, clamp) and apply into the OTHER x_pred buffer (Jacobi)
+//   density   (final)
+//   velocity  (x_pred - x_in) / dt
+//   xsph      XSPH viscosity, copy to state_out, apply_bounds      (fused)
+// As in the reference, the candidate set of every pass after the build is the
+// one binned at build time, queried from the particle's current position.
+#include "fs_internal.cuh"
+
+namespace fs {
+
+__global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
+                                const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
+                                float* __restrict__ mv, uint32_t* status);
+
+namespace {
+
+// predict_velocity_with_gravity (193-208) + predict_positions (212-224) +
+// apply_position_bounds (367-399); original order.
+__global__ void k_predict(int64_t n, fs_model m, const float* __restrict__ x, const float* __restrict__ v, float dt,
+                          Walls walls, float* __restrict__ x_pred, float* __restrict__ v_pred) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float3 p = ld3(x, i), u = ld3(v, i);
+  if (particle_pf(m.particle_flags, m.particle_mask, i) & PF_DYNAMIC) {
+    const float3 g = gravity_of(m, i);
+    u = make_float3(u.x + dt * g.x, u.y + dt * g.y, u.z + dt * g.z);
+    p = make_float3(p.x + dt * u.x, p.y + dt * u.y, p.z + dt * u.z);
+    clamp_position(walls, p);
+  }
+  st3(x_pred, i, p);
+  st3(v_pred, i, u);
+}
+
+__global__ void k_gather_xin(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ x,
+                             float4* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float3 p = ld3(x, perm[s]);
+  out[s] = make_float4(p.x, p.y, p.z, 0.f);
+}
+
+// compute_density (115-141), poly6, self included.
+__global__ void __launch_bounds__(kBlock) k_density(GridDev g, int64_t n, const float4* __restrict__ xs,
+                                                    const float* __restrict__ mv, float h, float* rho,
+                                                    float2* __restrict__ sc2) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 xi = xs[s];
+  const int32_t i = g.perm[s];
+  float acc = 0.f;
+  if (pf_of(xi) & PF_ACTIVE) {
+    const PbfK K(h);
+    const float h2m = h * h * 1.000002f;
+    for_each_candidate(g, xi.x, xi.y, xi.z, h, [&](int t) {
+      const float4 xj = __ldg(xs + t);
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r2 = dist2_rn(dx, dy, dz);
+      if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+      acc += __ldg(mv + t) * K.w(sqrtf(r2));
+    });
+  }
+  rho[i] = acc;
+  sc2[s] = make_float2(acc, 0.f);
+}
+
+// acceleration_non_pressure (145-189, PBF branches) + apply_non_pressure_prediction
+// (228-242) + apply_position_bounds; writes the updated x_pred to xs_out.
+struct AccelArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vs;
+  const float2* sc2;
+  fs_model m;
+  float h, particle_radius, dt;
+  Walls walls;
+  float* accel;
+  float4* xs_out;
+};
+
+__global__ void __launch_bounds__(kBlock) k_accel_apply(AccelArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const int32_t i = a.g.perm[s];
+  if (!(pf_of(xi) & PF_DYNAMIC)) {
+    st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
+    a.xs_out[s] = xi;
+    return;
+  }
+  const float4 vi = a.vs[s];
+  const float mu = a.m.viscosity[i];
+  const float gamma = a.m.surface_tension[i];
+  const float coh = gamma / vi.w;
+  const float visc_den_add = 0.01f * (a.h * a.h);
+  const PbfK K(a.h);
+  const float h2m = a.h * a.h * 1.000002f;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  if (gamma != 0.f || mu != 0.f) {
+    for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+      if (t == s) return;
+      const float4 xj = __ldg(a.xs + t);
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r2 = dist2_rn(dx, dy, dz);
+      if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+      const float4 vj = __ldg(a.vs + t);
+      const float r = sqrtf(r2);
+      float c = 0.f;
+      if (gamma != 0.f) c -= coh * vj.w * K.w(fmaxf(r, a.particle_radius));
+      if (mu != 0.f) {
+        const float vdot = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
+        if (vdot != 0.f) {
+          const float rho_j = __ldg(&a.sc2[t].x);
+          c += 10.f * mu * (vj.w / fmaxf(rho_j, 1.0e-6f)) * vdot / (r * r + visc_den_add) * K.dw_scale(r);
+        }
+      }
+      ax += c * dx;
+      ay += c * dy;
+      az += c * dz;
+    });
+  }
+  st3(a.accel, i, make_float3(ax, ay, az));
+  const float dvx = a.dt * ax, dvy = a.dt * ay, dvz = a.dt * az;
+  float3 p = make_float3(xi.x + a.dt * dvx, xi.y + a.dt * dvy, xi.z + a.dt * dvz);
+  clamp_position(a.walls, p);
+  a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
+}
+
+// compute_pbf_lambda (246-302)
+struct LambdaArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vs;   // .w = mass
+  const float* rest_density;
+  float h, eps;
+  int min_nb;
+  float* lam_s;       // cell order
+  float* lam;         // API
+  float* rho;         // API
+  int32_t* count;     // API
+};
+
+__global__ void __launch_bounds__(kBlock) k_lambda(LambdaArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const int32_t i = a.g.perm[s];
+  if (!(pf_of(xi) & PF_DYNAMIC)) {
+    a.lam_s[s] = 0.f;
+    if (a.lam) a.lam[i] = 0.f;
+    if (a.rho) a.rho[i] = 0.f;
+    if (a.count) a.count[i] = 0;
+    return;
+  }
+  const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
+  const PbfK K(a.h);
+  const float h2m = a.h * a.h * 1.000002f;
+  float rho = 0.f, sq = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+  int cnt = 0;
+  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+    const float4 xj = __ldg(a.xs + t);
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r2 = dist2_rn(dx, dy, dz);
+    if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+    const float r = sqrtf(r2);
+    if (t != s && r < a.h) ++cnt;
+    const float mj = __ldg(&a.vs[t].w);
+    rho += mj * K.w(r);
+    const float c = -(mj / rho0) * K.dw_scale(r);
+    const float gjx = c * dx, gjy = c * dy, gjz = c * dz;
+    sq += gjx * gjx + gjy * gjy + gjz * gjz;
+    gx -= gjx;
+    gy -= gjy;
+    gz -= gjz;
+  });
+  sq += gx * gx + gy * gy + gz * gz;
+  const float ci = fmaxf(rho / rho0 - 1.0f, 0.f);
+  const float l = (a.min_nb > 0 && cnt < a.min_nb) ? 0.f : -ci / (sq + a.eps);
+  a.lam_s[s] = l;
+  if (a.lam) a.lam[i] = l;
+  if (a.rho) a.rho[i] = rho;
+  if (a.count) a.count[i] = cnt;
+}
+
+// compute_delta_position + compute_scorr (306-350, 91-101), then
+// apply_delta_position (354-363) into xs_out (+ position bounds when asked).
+struct DeltaArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vs;   // .w = mass
+  const float* lam_s;
+  const float* rest_density;
+  float h, scorr_k, scorr_n, w_dq, max_dp;
+  int clamp;
+  Walls walls;
+  float* delta_p;     // API
+  float4* xs_out;     // may be null (separate-pass use)
+};
+
+__global__ void __launch_bounds__(kBlock) k_delta(DeltaArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const int32_t i = a.g.perm[s];
+  if (!(pf_of(xi) & PF_DYNAMIC)) {
+    st3(a.delta_p, i, make_float3(0.f, 0.f, 0.f));
+    if (a.xs_out) a.xs_out[s] = xi;
+    return;
+  }
+  const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
+  const float li = a.lam_s[s];
+  const PbfK K(a.h);
+  const float h2m = a.h * a.h * 1.000002f;
+  const bool scorr = a.scorr_k != 0.f && !(a.w_dq <= 1.0e-6f);
+  float dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
+  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+    if (t == s) return;
+    const float4 xj = __ldg(a.xs + t);
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r2 = dist2_rn(dx, dy, dz);
+    if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+    const float r = sqrtf(r2);
+    float sc = 0.f;
+    if (scorr) sc = -a.scorr_k * powf(K.w(r) / a.w_dq, a.scorr_n);
+    const float c = (li + __ldg(a.lam_s + t) + sc) * __ldg(&a.vs[t].w) * K.dw_scale(r);
+    dx_ += c * dx;
+    dy_ += c * dy;
+    dz_ += c * dz;
+  });
+  float3 d = make_float3(dx_ / rho0, dy_ / rho0, dz_ / rho0);
+  if (a.max_dp > 0.f) {
+    const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+    if (len > a.max_dp) {
+      const float sc = a.max_dp / fmaxf(len, 1.0e-12f);
+      d = make_float3(d.x * sc, d.y * sc, d.z * sc);
+    }
+  }
+  st3(a.delta_p, i, d);
+  if (a.xs_out) {
+    float3 p = make_float3(xi.x + d.x, xi.y + d.y, xi.z + d.z);
+    if (a.clamp) clamp_position(a.walls, p);
+    a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
+  }
+}
+
+// update_velocity_from_positions (403-416), cell order; .w keeps the mass
+__global__ void k_velocity(int64_t n, const float4* __restrict__ xs, const float4* __restrict__ xin,
+                           const float4* __restrict__ vs, float dt, float4* __restrict__ vout) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 xi = xs[s];
+  const float4 vi = vs[s];
+  float3 v = xyz(vi);  // non-dynamic: v_pred == v_in
+  if (pf_of(xi) & PF_DYNAMIC) {
+    const float4 x0 = xin[s];
+    const float d = fmaxf(dt, 1.0e-8f);
+    v = make_float3((xi.x - x0.x) / d, (xi.y - x0.y) / d, (xi.z - x0.z) / d);
+  }
+  vout[s] = make_float4(v.x, v.y, v.z, vi.w);
+}
+
+// apply_xsph_viscosity (435-463) + copy x_pred -> particle_q + apply_bounds (467-517)
+struct XsphArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vel;   // (v, mass) cell order
+  const float2* sc2;   // rho
+  float h, c;
+  Walls walls;
+  int bounds;          // fused apply_bounds (substep) or not (separate pass)
+  float* x_out;
+  float* v_out;
+  float* x_pred_api;   // optional
+};
+
+__global__ void __launch_bounds__(kBlock) k_xsph_final(XsphArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const float4 vi = a.vel[s];
+  const int32_t i = a.g.perm[s];
+  float3 v = xyz(vi);
+  float3 p = xyz(xi);
+  if (a.x_pred_api) st3(a.x_pred_api, i, p);
+  if (pf_of(xi) & PF_DYNAMIC) {
+    if (a.c > 0.f) {
+      const PbfK K(a.h);
+      const float h2m = a.h * a.h * 1.000002f;
+      float cx = 0.f, cy = 0.f, cz = 0.f;
+      for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+        if (t == s) return;
+        const float4 xj = __ldg(a.xs + t);
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = dist2_rn(dx, dy, dz);
+        if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+        const float4 vj = __ldg(a.vel + t);
+        const float w = (vj.w / fmaxf(__ldg(&a.sc2[t].x), 1.0e-6f)) * K.w(sqrtf(r2));
+        cx += (vj.x - vi.x) * w;
+        cy += (vj.y - vi.y) * w;
+        cz += (vj.z - vi.z) * w;
+      });
+      v = make_float3(vi.x + a.c * cx, vi.y + a.c * cy, vi.z + a.c * cz);
+    }
+    if (a.bounds) apply_walls(a.walls, p, v);
+  }
+  if (a.x_out) st3(a.x_out, i, p);
+  st3(a.v_out, i, v);
+}
+
+__global__ void k_scatter_x(int64_t n, const int32_t* __restrict__ perm, const float4* __restrict__ xs,
+                            float* __restrict__ x) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  st3(x, perm[s], xyz(xs[s]));
+}
+
+__global__ void k_gather_lambda(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
+                                float* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) out[s] = a[perm[s]];
+}
+
+__global__ void k_scalar_to_pair(int64_t n, const float* __restrict__ a, float2* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) out[s] = make_float2(a[s], 0.f);
+}
+
+int gather_pbf(fs_context* c, const fs_model* m, const float* x_in, cudaStream_t st) {
+  const int64_t n = m->n;
+  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, c->xo_tmp, c->vo_tmp, c->xs, c->vs, c->mv,
+                                                    c->status);
+  k_gather_xin<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, x_in, c->vs2);
+  return launch_check("pbf gather");
+}
+
+}  // namespace
+}  // namespace fs
+
+using namespace fs;
+
+extern "C" {
+
+int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so, const fs_pbf_params* p,
+                   float* accel, float* x_pred, fs_stream_t stream) {
+  if (!c || !m || !si || !so || !p) return set_error(FS_ERR_INVALID, "fs_pbf_substep: null argument");
+  if (m->n < 0) return set_error(FS_ERR_INVALID, "fs_pbf_substep: negative n");
+  if (m->n == 0) return FS_OK;
+  if (!m->particle_flags || !m->particle_mask || !m->particle_mass || !m->gravity || m->n_worlds < 1 ||
+      !m->rest_density || !m->viscosity || !m->surface_tension || !si->particle_q || !si->particle_qd ||
+      !so->particle_q || !so->particle_qd || !so->rho || !so->pbf_lambda || !so->neighbor_count || !so->delta_p ||
+      !accel)
+    return set_error(FS_ERR_INVALID, "fs_pbf_substep: missing array");
+  if (m->n > c->capacity) return set_error(FS_ERR_CAPACITY, "fs_pbf_substep: n > capacity");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n = m->n;
+  const float h = p->smoothing_length, dt = p->dt;
+  const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 2,
+                             p->particle_radius, p->boundary_epsilon);
+  int rc;
+  k_predict<<<blocks_for(n), kBlock, 0, st>>>(n, *m, si->particle_q, si->particle_qd, dt, w, c->xo_tmp, c->vo_tmp);
+  if ((rc = launch_check("pbf predict"))) return rc;
+  if ((rc = grid_build(c, c->xo_tmp, n, h, st))) return rc;
+  if ((rc = gather_pbf(c, m, si->particle_q, st))) return rc;
+  const GridDev g = grid_view(c);
+  k_density<<<blocks_for(n), kBlock, 0, st>>>(g, n, c->xs, c->mv, h, so->rho, c->sc2);
+  AccelArgs aa;
+  aa.g = g;
+  aa.n = n;
+  aa.xs = c->xs;
+  aa.vs = c->vs;
+  aa.sc2 = c->sc2;
+  aa.m = *m;
+  aa.h = h;
+  aa.particle_radius = p->particle_radius;
+  aa.dt = dt;
+  aa.walls = w;
+  aa.accel = accel;
+  aa.xs_out = c->xs2;
+  k_accel_apply<<<blocks_for(n), kBlock, 0, st>>>(aa);
+  if ((rc = launch_check("pbf accel"))) return rc;
+  float4* cur = c->xs2;
+  float4* nxt = c->xs;
+  for (int it = 0; it < p->max_iterations; ++it) {
+    const GridDev gi = grid_view(c);
+    LambdaArgs la;
+    la.g = gi;
+    la.n = n;
+    la.xs = cur;
+    la.vs = c->vs;
+    la.rest_density = m->rest_density;
+    la.h = h;
+    la.eps = p->lambda_epsilon;
+    la.min_nb = p->min_neighbors_for_lambda;
+    la.lam_s = c->sc1;
+    la.lam = so->pbf_lambda;
+    la.rho = so->rho;
+    la.count = so->neighbor_count;
+    k_lambda<<<blocks_for(n), kBlock, 0, st>>>(la);
+    DeltaArgs da;
+    da.g = gi;
+    da.n = n;
+    da.xs = cur;
+    da.vs = c->vs;
+    da.lam_s = c->sc1;
+    da.rest_density = m->rest_density;
+    da.h = h;
+    da.scorr_k = p->scorr_k;
+    da.scorr_n = p->scorr_n;
+    da.w_dq = p->scorr_w_delta_q;
+    da.max_dp = p->max_delta_position;
+    da.clamp = (p->rebuild_grid_each_iteration || it == p->max_iterations - 1) ? 1 : 0;
+    da.walls = w;
+    da.delta_p = so->delta_p;
+    da.xs_out = nxt;
+    k_delta<<<blocks_for(n), kBlock, 0, st>>>(da);
+    if ((rc = launch_check("pbf iteration"))) return rc;
+    float4* t = cur;
+    cur = nxt;
+    nxt = t;
+    if (p->rebuild_grid_each_iteration) {
+      // x_pred back to original order, rebuild, regather (v_pred/x_in follow)
+      k_scatter_x<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, cur, c->xo_tmp);
+      if ((rc = grid_build(c, c->xo_tmp, n, h, st))) return rc;
+      if ((rc = gather_pbf(c, m, si->particle_q, st))) return rc;
+      cur = c->xs;
+      nxt = c->xs2;
+    }
+  }
+  // final density on the bounded x_pred (bounds were fused into the last apply)
+  const GridDev gf = grid_view(c);
+  k_density<<<blocks_for(n), kBlock, 0, st>>>(gf, n, cur, c->mv, h, so->rho, c->sc2);
+  k_velocity<<<blocks_for(n), kBlock, 0, st>>>(n, cur, c->vs2, c->vs, dt, nxt);
+  XsphArgs xa;
+  xa.g = gf;
+  xa.n = n;
+  xa.xs = cur;
+  xa.vel = nxt;
+  xa.sc2 = c->sc2;
+  xa.h = h;
+  xa.c = p->xsph_c;
+  xa.walls = w;
+  xa.bounds = 1;
+  xa.x_out = so->particle_q;
+  xa.v_out = so->particle_qd;
+  xa.x_pred_api = x_pred;
+  k_xsph_final<<<blocks_for(n), kBlock, 0, st>>>(xa);
+  c->last_stream = st;
+  return launch_check("pbf final");
+}
+
+int fs_pbf_density(fs_context* c, const fs_model* m, const float* x, float h, float* rho, fs_stream_t stream) {
+  if (!c || !m || !x || !rho) return set_error(FS_ERR_INVALID, "fs_pbf_density: null argument");
+  if (m->n == 0) return FS_OK;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_pbf_density: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, nullptr, c->xs, nullptr, c->mv,
+                                                       c->status);
+  k_density<<<blocks_for(m->n), kBlock, 0, st>>>(grid_view(c), m->n, c->xs, c->mv, h, rho, c->sc2);
+  return launch_check("fs_pbf_density");
+}
+
+int fs_pbf_lambda(fs_context* c, const fs_model* m, const float* x_pred, const fs_pbf_params* p, float* pbf_lambda,
+                  float* rho, int32_t* neighbor_count, fs_stream_t stream) {
+  if (!c || !m || !x_pred || !p || !pbf_lambda) return set_error(FS_ERR_INVALID, "fs_pbf_lambda: null argument");
+  if (m->n == 0) return FS_OK;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_pbf_lambda: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, x_pred, c->xs, c->vs, nullptr,
+                                                       c->status);
+  LambdaArgs la;
+  la.g = grid_view(c);
+  la.n = m->n;
+  la.xs = c->xs;
+  la.vs = c->vs;
+  la.rest_density = m->rest_density;
+  la.h = p->smoothing_length;
+  la.eps = p->lambda_epsilon;
+  la.min_nb = p->min_neighbors_for_lambda;
+  la.lam_s = c->sc1;
+  la.lam = pbf_lambda;
+  la.rho = rho;
+  la.count = neighbor_count;
+  k_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(la);
+  return launch_check("fs_pbf_lambda");
+}
+
+int fs_pbf_delta(fs_context* c, const fs_model* m, const float* x_pred, const float* pbf_lambda,
+                 const fs_pbf_params* p, float* delta_p, fs_stream_t stream) {
+  if (!c || !m || !x_pred || !pbf_lambda || !p || !delta_p)
+    return set_error(FS_ERR_INVALID, "fs_pbf_delta: null argument");
+  if (m->n == 0) return FS_OK;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_pbf_delta: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, x_pred, c->xs, c->vs, nullptr,
+                                                       c->status);
+  k_gather_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, pbf_lambda, c->sc1);
+  DeltaArgs da;
+  da.g = grid_view(c);
+  da.n = m->n;
+  da.xs = c->xs;
+  da.vs = c->vs;
+  da.lam_s = c->sc1;
+  da.rest_density = m->rest_density;
+  da.h = p->smoothing_length;
+  da.scorr_k = p->scorr_k;
+  da.scorr_n = p->scorr_n;
+  da.w_dq = p->scorr_w_delta_q;
+  da.max_dp = p->max_delta_position;
+  da.clamp = 0;
+  da.walls = Walls{};
+  da.delta_p = delta_p;
+  da.xs_out = nullptr;
+  k_delta<<<blocks_for(m->n), kBlock, 0, st>>>(da);
+  return launch_check("fs_pbf_delta");
+}
+
+int fs_pbf_xsph(fs_context* c, const fs_model* m, const float* x_pred, const float* v_in, const float* rho, float h,
+                float xsph_c, float* v_out, fs_stream_t stream) {
+  if (!c || !m || !x_pred || !v_in || !rho || !v_out) return set_error(FS_ERR_INVALID, "fs_pbf_xsph: null argument");
+  if (m->n == 0) return FS_OK;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_pbf_xsph: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, v_in, c->xs, c->vs2, nullptr,
+                                                       c->status);
+  k_gather_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, rho, c->sc1);
+  k_scalar_to_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->sc1, c->sc2);
+  XsphArgs xa;
+  xa.g = grid_view(c);
+  xa.n = m->n;
+  xa.xs = c->xs;
+  xa.vel = c->vs2;
+  xa.sc2 = c->sc2;
+  xa.h = h;
+  xa.c = xsph_c;
+  xa.walls = Walls{};
+  xa.bounds = 0;
+  xa.x_out = nullptr;
+  xa.v_out = v_out;
+  xa.x_pred_api = nullptr;
+  k_xsph_final<<<blocks_for(m->n), kBlock, 0, st>>>(xa);
+  return launch_check("fs_pbf_xsph");
+}
+
+}  // extern "C"

@@ -1,0 +1,282 @@
+// WCSPH substep on B200 (replaces SolverWCSPH.step, solver_wcsph.py:431-535).
+//
+// Pass structure (one thread per cell-sorted slot; neighbour reads are
+// contiguous slot ranges of the cell-sorted streams):
+//   grid build(x_in)                       -- fs_grid.cu
+//   gather    x_in, v_in, mass, flags      -> xs, vs, mv     (cell order)
+//   density   rho, p (EOS)                 -> sc2 (cell order) + rho/pressure (original order)
+//   force     pressure + viscosity + cohesion + gravity, then
+//             integrate_velocity, integrate_positions and apply_bounds fused
+//             -> accel, particle_qd, particle_q (original order)
+#include "fs_internal.cuh"
+
+namespace fs {
+
+// -------------------------------------------------------------- gather ----
+// Cell-order copies of what neighbour loops read.  mv = rest_density * volume
+// with volume = mass / max(rest_density, 1e-6) (compute_particle_volume,
+// solver_wcsph.py:110-116).
+__global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
+                                const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
+                                float* __restrict__ mv, uint32_t* status) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int32_t i = perm[s];
+  const float3 p = ld3(x, i);
+  const int pf = particle_pf(m.particle_flags, m.particle_mask, i);
+  xs[s] = make_float4(p.x, p.y, p.z, pack_pf(pf));
+  const float mass = m.particle_mass[i];
+  if (vs) {
+    const float3 u = ld3(v, i);
+    vs[s] = make_float4(u.x, u.y, u.z, mass);
+  }
+  if (mv) {
+    const float rd = m.rest_density[i];
+    mv[s] = rd * (mass / fmaxf(rd, 1.0e-6f));
+  }
+  if (m.particle_world) {
+    const int w = m.particle_world[i];
+    if (w >= m.n_worlds) atomicOr(status, FS_STATUS_BOUNDS);
+  }
+}
+
+// ------------------------------------------------------------- density ----
+// compute_density_pressure, solver_wcsph.py:120-158.  Self included.
+struct DensityArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float* mv;
+  const float* rest_density;  // original order
+  const float* stiffness;     // original order (nullptr: density only)
+  const float* exponent;
+  float h;
+  int clamp;
+  float* rho;                 // original order (API)
+  float* pressure;            // original order (API), may be null
+  float2* sc2;                // cell order (rho, p)
+};
+
+__global__ void __launch_bounds__(kBlock) k_wcsph_density(DensityArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const int32_t i = a.g.perm[s];
+  if (!(pf_of(xi) & PF_ACTIVE)) {
+    a.rho[i] = 0.f;
+    if (a.pressure) a.pressure[i] = 0.f;
+    a.sc2[s] = make_float2(0.f, 0.f);
+    return;
+  }
+  const CubicK K(a.h);
+  const float h2 = a.h * a.h;
+  float acc = 0.f;
+  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+    const float4 xj = __ldg(a.xs + t);
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r2 = dist2_rn(dx, dy, dz);
+    if (r2 > h2 || !(pf_of(xj) & PF_ACTIVE)) return;  // W = 0 beyond the support
+    acc += __ldg(a.mv + t) * K.w(sqrtf(r2));
+  });
+  float p = 0.f;
+  if (a.stiffness) {
+    p = a.stiffness[i] * (powf(acc / fmaxf(a.rest_density[i], 1.0e-6f), a.exponent[i]) - 1.0f);
+    if (a.clamp) p = fmaxf(p, 0.f);
+    a.pressure[i] = p;
+  }
+  a.rho[i] = acc;
+  a.sc2[s] = make_float2(acc, p);
+}
+
+// --------------------------------------------------------------- force ----
+// acceleration_wcsph (162-228) + integrate_velocity (232-244) +
+// integrate_positions (248-260) + apply_bounds (264-305).
+struct ForceArgs {
+  GridDev g;
+  int64_t n;
+  const float4* xs;
+  const float4* vs;
+  const float2* sc2;
+  fs_model m;
+  float h, particle_radius, dt;
+  Walls walls;
+  float* accel;
+  float* x_out;
+  float* v_out;
+};
+
+__global__ void __launch_bounds__(kBlock) k_wcsph_force(ForceArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const float4 xi = a.xs[s];
+  const float4 vi = a.vs[s];
+  const int32_t i = a.g.perm[s];
+  if (!(pf_of(xi) & PF_DYNAMIC)) {
+    st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
+    st3(a.v_out, i, xyz(vi));
+    st3(a.x_out, i, xyz(xi));
+    return;
+  }
+  const float2 rp = a.sc2[s];
+  const float rho_i = rp.x, p_i = rp.y;
+  const float m_i = vi.w;
+  const float mu = a.m.viscosity[i];
+  const float gamma = a.m.surface_tension[i];
+  const float dp_i = p_i / fmaxf(rho_i * rho_i, 1.0e-6f);
+  const float coh = gamma / m_i;
+  const float visc_den_add = 0.01f * (a.h * a.h);
+  const CubicK K(a.h);
+  const float h2 = a.h * a.h;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
+    if (t == s) return;
+    const float4 xj = __ldg(a.xs + t);
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r2 = dist2_rn(dx, dy, dz);
+    if (r2 > h2 || !(pf_of(xj) & PF_ACTIVE)) return;  // every term vanishes beyond h
+    const float4 vj = __ldg(a.vs + t);
+    const float2 rpj = __ldg(a.sc2 + t);
+    const float r = sqrtf(r2);
+    const float m_j = vj.w;
+    // cohesion: -gamma/m_i * m_j * d * W(max(r, r_p))
+    const float wc = coh * m_j * K.w(fmaxf(r, a.particle_radius));
+    // viscosity: 10 mu (m_j / max(rho_j,1e-6)) (v_ij . d) / (r^2 + 0.01 h^2) * gradW
+    const float vdot = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
+    const float gs = K.dw_scale(r);
+    const float visc = 10.f * mu * (m_j / fmaxf(rpj.x, 1.0e-6f)) * vdot / (r * r + visc_den_add);
+    // pressure: -m_j (p_i/rho_i^2 + p_j/rho_j^2) gradW
+    const float dp_j = rpj.y / fmaxf(rpj.x * rpj.x, 1.0e-6f);
+    const float pres = -m_j * (dp_i + dp_j);
+    const float c = (visc + pres) * gs - wc;
+    ax += c * dx;
+    ay += c * dy;
+    az += c * dz;
+  });
+  const float3 g = gravity_of(a.m, i);
+  const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
+  st3(a.accel, i, acc);
+  float3 v = make_float3(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z);
+  float3 p = make_float3(xi.x + v.x * a.dt, xi.y + v.y * a.dt, xi.z + v.z * a.dt);
+  apply_walls(a.walls, p, v);
+  st3(a.v_out, i, v);
+  st3(a.x_out, i, p);
+}
+
+// (a[i], b[i]) of original order into cell order
+__global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
+                              const float* __restrict__ b, float2* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int32_t i = perm[s];
+  out[s] = make_float2(a[i], b ? b[i] : 0.f);
+}
+
+int wcsph_gather(fs_context* c, const fs_model* m, const float* x, const float* v, cudaStream_t st) {
+  const int64_t n = m->n;
+  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, x, v, c->xs, c->vs, c->mv, c->status);
+  return launch_check("wcsph gather");
+}
+
+int launch_density(fs_context* c, const fs_model* m, float h, int clamp, bool eos, float* rho, float* pressure,
+                   cudaStream_t st) {
+  DensityArgs a;
+  a.g = grid_view(c);
+  a.n = m->n;
+  a.xs = c->xs;
+  a.mv = c->mv;
+  a.rest_density = m->rest_density;
+  a.stiffness = eos ? m->stiffness : nullptr;
+  a.exponent = m->exponent;
+  a.h = h;
+  a.clamp = clamp;
+  a.rho = rho;
+  a.pressure = pressure;
+  a.sc2 = c->sc2;
+  k_wcsph_density<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  return launch_check("wcsph density");
+}
+
+int launch_force(fs_context* c, const fs_model* m, const fs_wcsph_params* p, float* accel, float* x_out,
+                 float* v_out, cudaStream_t st) {
+  ForceArgs a;
+  a.g = grid_view(c);
+  a.n = m->n;
+  a.xs = c->xs;
+  a.vs = c->vs;
+  a.sc2 = c->sc2;
+  a.m = *m;
+  a.h = p->smoothing_length;
+  a.particle_radius = p->particle_radius;
+  a.dt = p->dt;
+  a.walls = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 0, 0.f, 0.f);
+  a.accel = accel;
+  a.x_out = x_out;
+  a.v_out = v_out;
+  k_wcsph_force<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  return launch_check("wcsph force");
+}
+
+int validate_model(const fs_model* m, bool wcsph) {
+  if (!m || m->n < 0) return set_error(FS_ERR_INVALID, "model: null or negative n");
+  if (m->n == 0) return FS_OK;
+  if (!m->particle_flags || !m->particle_mass || !m->gravity || m->n_worlds < 1 || !m->rest_density)
+    return set_error(FS_ERR_INVALID, "model: missing particle_flags/particle_mass/gravity/rest_density");
+  if (wcsph && (!m->stiffness || !m->exponent))
+    return set_error(FS_ERR_INVALID, "model: WCSPH needs stiffness and exponent");
+  return FS_OK;
+}
+
+}  // namespace fs
+
+using namespace fs;
+
+extern "C" {
+
+int fs_wcsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so, const fs_wcsph_params* p,
+                     float* accel, fs_stream_t stream) {
+  if (!c || !si || !so || !p) return set_error(FS_ERR_INVALID, "fs_wcsph_substep: null argument");
+  int rc = validate_model(m, true);
+  if (rc) return rc;
+  if (m->n == 0) return FS_OK;
+  if (!m->particle_mask || !m->viscosity || !m->surface_tension || !si->particle_q || !si->particle_qd ||
+      !so->particle_q || !so->particle_qd || !so->rho || !so->pressure || !accel)
+    return set_error(FS_ERR_INVALID, "fs_wcsph_substep: missing array");
+  if (m->n > c->capacity) return set_error(FS_ERR_CAPACITY, "fs_wcsph_substep: n > capacity");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const float h = p->smoothing_length;
+  if ((rc = grid_build(c, si->particle_q, m->n, h, st))) return rc;
+  if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
+  if ((rc = launch_density(c, m, h, p->clamp_negative_pressure, true, so->rho, so->pressure, st))) return rc;
+  return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st);
+}
+
+int fs_wcsph_density(fs_context* c, const fs_model* m, const float* x, float h, int32_t clamp_negative, float* rho,
+                     float* pressure, fs_stream_t stream) {
+  if (!c || !x || !rho || !pressure) return set_error(FS_ERR_INVALID, "fs_wcsph_density: null argument");
+  int rc = validate_model(m, true);
+  if (rc || m->n == 0) return rc;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_wcsph_density: build the grid for these points first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, nullptr, c->xs, nullptr, c->mv,
+                                                       c->status);
+  return launch_density(c, m, h, clamp_negative, true, rho, pressure, st);
+}
+
+int fs_wcsph_force_integrate(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so,
+                             const fs_wcsph_params* p, float* accel, fs_stream_t stream) {
+  if (!c || !si || !so || !p || !accel) return set_error(FS_ERR_INVALID, "fs_wcsph_force_integrate: null argument");
+  int rc = validate_model(m, true);
+  if (rc || m->n == 0) return rc;
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_wcsph_force_integrate: build the grid first");
+  if (!so->rho || !so->pressure) return set_error(FS_ERR_INVALID, "fs_wcsph_force_integrate: needs state_out rho/p");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
+  k_gather_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, so->rho, so->pressure, c->sc2);
+  if ((rc = launch_check("wcsph gather rho/p"))) return rc;
+  return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st);
+}
+
+}  // extern "C"

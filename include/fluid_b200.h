@@ -1,0 +1,212 @@
+/* fluid_b200.h — C ABI of the B200 particle-fluid library (libfluid_b200.so).
+ *
+ * Drop-in replacement for the hot path of SParksLz/fluid_simulation: the
+ * warp-lang 1.17.0 hash grid (`wp.HashGrid`) and the per-particle kernels of
+ * SolverWCSPH / SolverDFSPH / SolverPBF behind
+ * `SolverBase.step(state_in, state_out, control, contacts, dt)`.
+ *
+ * Conventions
+ *  - Every array is a raw DEVICE pointer into caller-owned memory laid out as
+ *    the reference's Newton arrays: vec3 arrays are float[n][3] (AoS), scalars
+ *    float[n], flags/masks/worlds/counts int32[n], all in ORIGINAL particle
+ *    order.  The library never frees caller memory.
+ *  - Scratch (cell tables, cell-sorted copies, reductions) belongs to an
+ *    fs_context, which is bound to one device and sized for `capacity`
+ *    particles at creation.
+ *  - Every call is asynchronous on `stream` (a cudaStream_t; NULL = legacy
+ *    default stream) and returns an int status: FS_OK or one of FS_ERR_*.
+ *    Kernel-side conditions are recorded in the context's status word
+ *    (FS_STATUS_* bits) and read with fs_status_read.
+ *  - Errors never trap or hang the device.
+ */
+#ifndef FLUID_B200_H
+#define FLUID_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* fs_stream_t; /* == cudaStream_t */
+typedef struct fs_context fs_context;
+
+/* return codes */
+#define FS_OK 0
+#define FS_ERR_INVALID 1   /* null pointer, negative size, bad config */
+#define FS_ERR_CUDA 2      /* a CUDA runtime call failed (fs_last_error_string) */
+#define FS_ERR_CAPACITY 3  /* n exceeds the context capacity */
+#define FS_ERR_NOGRID 4    /* a pass needs a grid that was not built for this n */
+
+/* device status word bits (sticky until fs_status_clear) */
+#define FS_STATUS_NONFINITE 1u      /* a non-finite position reached the grid build */
+#define FS_STATUS_GRID_OVERFLOW 2u  /* more particles than the grid was reserved for */
+#define FS_STATUS_BOUNDS 4u         /* a checked index fell outside its array */
+#define FS_STATUS_TIMEOUT 8u        /* a bounded device-side wait gave up */
+
+/* Hash-grid geometry.  The reference uses wp.HashGrid(128, 128, 128)
+ * (solver_wcsph.py:398-402) with cell width = support radius h and warp's
+ * truncating float-to-int conversion (rounding = 0).  rounding = 1 selects
+ * floor.  Cell coords wrap modulo the dims (shifted by 2^20 first). */
+typedef struct {
+  int32_t dim_x, dim_y, dim_z;
+  int32_t rounding;
+} fs_grid_config;
+
+/* Model arrays (Newton Model + the `sph` custom-attribute namespace).
+ * Unused fields may be NULL (stiffness/exponent are WCSPH only). */
+typedef struct {
+  int64_t n;                      /* Model.particle_count */
+  int32_t n_worlds;               /* rows of gravity */
+  const int32_t* particle_flags;  /* Model.particle_flags (bit 0 = ParticleFlags.ACTIVE) */
+  const int32_t* particle_mask;   /* Model.sph.particle_mask (non-zero = not dynamic) */
+  const int32_t* particle_world;  /* Model.particle_world (may be NULL = world 0) */
+  const float* particle_mass;     /* Model.particle_mass */
+  const float* gravity;           /* Model.gravity [n_worlds][3] */
+  const float* rest_density;      /* Model.sph.rest_density */
+  const float* surface_tension;   /* Model.sph.surface_tension (cohesion coefficient) */
+  const float* viscosity;         /* Model.sph.viscosity */
+  const float* stiffness;         /* Model.sph.stiffness (WCSPH) */
+  const float* exponent;          /* Model.sph.exponent (WCSPH) */
+} fs_model;
+
+/* One Newton State: particle_q / particle_qd plus the `sph` STATE attributes.
+ * Fields a solver does not write may be NULL. */
+typedef struct {
+  float* particle_q;      /* [n][3] */
+  float* particle_qd;     /* [n][3] */
+  float* rho;             /* all solvers */
+  float* pressure;        /* WCSPH */
+  float* factor;          /* DFSPH */
+  float* rho_star;        /* DFSPH */
+  float* d_rho_dt;        /* DFSPH */
+  float* kappa;           /* DFSPH */
+  float* kappa_v;         /* DFSPH */
+  int32_t* neighbor_count;/* DFSPH, PBF */
+  float* v_star;          /* DFSPH [n][3] */
+  float* pbf_lambda;      /* PBF */
+  float* delta_p;         /* PBF [n][3] */
+} fs_state;
+
+/* Scalars of one WCSPH substep (SolverWCSPH.SphConfig, solver_wcsph.py:309-318). */
+typedef struct {
+  float dt;
+  float smoothing_length;  /* h = particle_length * smoothing_length_coff */
+  float particle_radius;   /* config radius, or Model.particle_max_radius when <= 0 */
+  float bound_width, bound_height, bound_length;
+  float boundary_damping;
+  int32_t clamp_negative_pressure;
+} fs_wcsph_params;
+
+/* Scalars of one DFSPH substep (SolverDFSPH.SphConfig, solver_dfsph.py:446-463). */
+typedef struct {
+  float dt;
+  float smoothing_length;
+  float particle_radius;
+  float bound_width, bound_height, bound_length;
+  float boundary_damping;
+  int32_t max_rho_iterations, max_vel_iterations, warm_start, min_neighbors_for_factor;
+  float eta_density, eta_divergence, max_kappa, max_kappa_v;
+} fs_dfsph_params;
+
+/* Scalars of one PBF substep (SolverPBF.PbfConfig, solver_pbf.py:521-539). */
+typedef struct {
+  float dt;
+  float smoothing_length;
+  float particle_radius;
+  float bound_width, bound_height, bound_length;
+  float boundary_damping, boundary_epsilon;
+  int32_t max_iterations, min_neighbors_for_lambda, rebuild_grid_each_iteration;
+  float lambda_epsilon, scorr_k, scorr_n, scorr_w_delta_q, max_delta_position, xsph_c;
+} fs_pbf_params;
+
+/* Per-step DFSPH solver record (read back on demand; not needed to step). */
+typedef struct {
+  int32_t rho_iterations;       /* density iterations entered */
+  int32_t vel_iterations;       /* divergence iterations entered */
+  double density_residual;      /* last computed mean max(rho*-rho0, 0) */
+  double divergence_residual;   /* last computed mean max(drho/dt, 0) */
+} fs_dfsph_info;
+
+/* ---- context / grid ---------------------------------------------------
+ * Replaces `wp.HashGrid(128,128,128)` + `.reserve(N)` done by every solver
+ * constructor (solver_wcsph.py:398-402, solver_dfsph.py:541-545,
+ * solver_pbf.py:634-638) and the solvers' private scratch arrays. */
+int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* grid, int32_t device);
+int fs_context_destroy(fs_context* ctx);
+int64_t fs_context_capacity(const fs_context* ctx);
+
+/* `grid.build(points, radius)` (solver_wcsph.py:456, solver_dfsph.py:624,783,
+ * solver_pbf.py:737,858): cell keys, stable sort by cell, cell ranges. */
+int fs_grid_build(fs_context* ctx, const float* x, int64_t n, float radius, fs_stream_t stream);
+
+/* Copies of the last build's tables into caller device arrays (tests):
+ * point_ids[n] (`hash_grid_point_id`), point_cells[n] (sorted cell keys),
+ * cell_starts/cell_ends[dim_x*dim_y*dim_z] (empty cells: start == end). */
+int fs_grid_tables(fs_context* ctx, int32_t* point_ids, int32_t* point_cells, int32_t* cell_starts,
+                   int32_t* cell_ends, fs_stream_t stream);
+
+/* Candidate enumeration of `wp.hash_grid_query(grid, q[i], r)` against the
+ * last build (tests): counts[i], and when cand != NULL the candidates in
+ * visiting order at cand[offsets[i]...]. */
+int fs_grid_candidates(fs_context* ctx, const float* q, int64_t nq, float r, int64_t* counts,
+                       const int64_t* offsets, int32_t* cand, fs_stream_t stream);
+
+/* ---- whole substeps --------------------------------------------------- */
+/* SolverWCSPH.step (solver_wcsph.py:431-535).  accel = solver._particle_accel [n][3]. */
+int fs_wcsph_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
+                     const fs_wcsph_params* params, float* accel, fs_stream_t stream);
+/* SolverDFSPH.step (solver_dfsph.py:598-898).  Iteration decisions are taken
+ * on the device (no host synchronisation inside the step). */
+int fs_dfsph_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
+                     const fs_dfsph_params* params, float* accel, fs_stream_t stream);
+int fs_dfsph_info_read(fs_context* ctx, fs_dfsph_info* info); /* synchronises the context's last stream */
+/* SolverPBF.step (solver_pbf.py:676-954).  x_pred may be NULL (solver._x_pred [n][3]). */
+int fs_pbf_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
+                   const fs_pbf_params* params, float* accel, float* x_pred, fs_stream_t stream);
+
+/* ---- separate passes (each needs fs_grid_build(positions, h) first) --------
+ * WCSPH compute_density_pressure (solver_wcsph.py:120-158). */
+int fs_wcsph_density(fs_context* ctx, const fs_model* model, const float* x, float h, int32_t clamp_negative,
+                     float* rho, float* pressure, fs_stream_t stream);
+/* WCSPH acceleration_wcsph + integrate_velocity + integrate_positions +
+ * apply_bounds (solver_wcsph.py:162-305), fused. */
+int fs_wcsph_force_integrate(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
+                             const fs_wcsph_params* params, float* accel, fs_stream_t stream);
+/* DFSPH compute_density + compute_factor_dfsph (solver_dfsph.py:107-174), fused. */
+int fs_dfsph_density_factor(fs_context* ctx, const fs_model* model, const float* x, float h,
+                            int32_t min_neighbors_for_factor, float* rho, float* factor, int32_t* neighbor_count,
+                            fs_stream_t stream);
+/* DFSPH compute_density_change_rate (solver_dfsph.py:246-272). */
+int fs_dfsph_divergence(fs_context* ctx, const fs_model* model, const float* x, const float* v, float h,
+                        float* d_rho_dt, fs_stream_t stream);
+/* DFSPH apply_constant_density_correction / apply_divergence_free_correction
+ * (solver_dfsph.py:310-337, 376-403): v_star[i] -= dt * sum(...), in place. */
+int fs_dfsph_correct(fs_context* ctx, const fs_model* model, const float* x, float* v_star, const float* rho,
+                     const float* kappa, float h, float dt, fs_stream_t stream);
+/* DFSPH residual (solver_dfsph.py:579-596): mean over dynamic particles of
+ * max(a - b, 0) (b may be NULL), written as one double to *out (device). */
+int fs_dfsph_residual(fs_context* ctx, const fs_model* model, const float* a, const float* b, double* out,
+                      fs_stream_t stream);
+/* PBF compute_density (poly6, solver_pbf.py:115-141). */
+int fs_pbf_density(fs_context* ctx, const fs_model* model, const float* x, float h, float* rho, fs_stream_t stream);
+/* PBF compute_pbf_lambda (solver_pbf.py:246-302). */
+int fs_pbf_lambda(fs_context* ctx, const fs_model* model, const float* x_pred, const fs_pbf_params* params,
+                  float* pbf_lambda, float* rho, int32_t* neighbor_count, fs_stream_t stream);
+/* PBF compute_delta_position + compute_scorr (solver_pbf.py:306-350, 91-101). */
+int fs_pbf_delta(fs_context* ctx, const fs_model* model, const float* x_pred, const float* pbf_lambda,
+                 const fs_pbf_params* params, float* delta_p, fs_stream_t stream);
+/* PBF apply_xsph_viscosity (solver_pbf.py:435-463). */
+int fs_pbf_xsph(fs_context* ctx, const fs_model* model, const float* x_pred, const float* v_in, const float* rho,
+                float h, float xsph_c, float* v_out, fs_stream_t stream);
+
+/* ---- status ------------------------------------------------------------ */
+int fs_status_read(fs_context* ctx, uint32_t* status); /* synchronises the context's last stream */
+int fs_status_clear(fs_context* ctx, fs_stream_t stream);
+const char* fs_last_error_string(void);
+const char* fs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLUID_B200_H */

@@ -223,8 +223,8 @@ def main():
                                   particle_length=d, smoothing_length_coff=2.0, boundary_damping=-0.3, **box)
         run_case(wp, "pbf_block", SolverPBF, cfg, blk, pb_mat, 1.0 / 240.0, pnames)
     if want("pbf_block_scorr"):
-        cfg = SolverPBF.PbfConfig(max_iterations=3, lambda_epsilon=10.0, min_neighbors_for_lambda=0, scorr_k=1.0e-2,
-                                  scorr_n=4.0, scorr_q=0.3, max_delta_position=0.0, xsph_c=0.01,
+        cfg = SolverPBF.PbfConfig(max_iterations=3, lambda_epsilon=100.0, min_neighbors_for_lambda=0, scorr_k=1.0e-3,
+                                  scorr_n=4.0, scorr_q=0.3, max_delta_position=0.5 * d, xsph_c=0.01,
                                   particle_radius=0.5 * d, particle_length=d, smoothing_length_coff=2.0,
                                   boundary_damping=-0.2, boundary_epsilon=1.0e-4,
                                   rebuild_grid_each_iteration=True, **box)

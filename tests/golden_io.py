@@ -30,9 +30,33 @@ def solver_of(name):
     return name.split("_")[0]
 
 
-def rel_err(a, b):
-    """max |a-b| / max(|b|) over the array (a norm-relative error)."""
+def rel_err(a, b, scale=None):
+    """max |a-b| / max(|b|) over the array (a norm-relative error); ``scale``
+    replaces max(|b|) for quantities formed by cancellation."""
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
-    scale = max(float(np.abs(b).max()) if b.size else 0.0, 1e-30)
-    return float(np.abs(a - b).max()) / scale if b.size else 0.0
+    if not b.size:
+        return 0.0
+    s = float(np.abs(b).max()) if scale is None else float(scale)
+    return float(np.abs(a - b).max()) / max(s, 1e-30)
+
+
+def field_scale(name, ref_sph, dt):
+    """Natural magnitude of a derived field, or None for max |field|.
+
+    kappa_v = min((1/dt) max(drho/dt, 0) rho factor, cap): near convergence the
+    positive part of drho/dt is orders of magnitude below |drho/dt| itself, so
+    its FP32 error is measured against (1/dt) |rho factor drho/dt|."""
+    if name == "kappa_v" and {"rho", "factor", "d_rho_dt"} <= set(ref_sph):
+        r = np.asarray(ref_sph["rho"], np.float64) * np.asarray(ref_sph["factor"], np.float64)
+        return float(np.abs(r * np.asarray(ref_sph["d_rho_dt"], np.float64)).max()) / dt
+    return None
+
+
+def velocity_scale(v_ref, x_ref, dt, tol):
+    """PBF sets v = (x_pred - x_in) / dt: a difference of O(|x|) positions, so a
+    few-ulp position difference becomes eps32 |x| / dt in v.  The scale keeps
+    the tolerance at tol relative to |v| but never below 4 ulp(|x|) / dt."""
+    vmax = float(np.abs(v_ref).max())
+    xmax = float(np.abs(x_ref).max())
+    return max(vmax, 4.0 * float(np.finfo(np.float32).eps) * xmax / (dt * tol))
