@@ -1,0 +1,413 @@
+"""Benchmark of the particle-fluid hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Metric: particle-steps/s (one particle advanced one solver substep).
+Headline workload (default ``pbf_dam_401856``): the reference's PBF dam
+break at 401,856 particles (make_scene(400000)), its harness config (4
+constraint iterations, lambda_eps 100, min 8 neighbours, s_corr off, dx clamp
+r/2, XSPH 0.05) at the fixed substep dt = 1/240 s.  That is the workload of
+the only published solve time (64.65 ms per 4-substep frame on an RTX 4090,
+24.86 M particle-substeps/s).  A "step" is one solver substep.
+
+* value: device time with CUDA events around every timed step, L2 flushed by
+  a 512 MB write between steps (outside the events); inputs resident in HBM.
+* e2e: the same metric through the drop-in solver API with host state:
+  every step copies particle_q / particle_qd from pinned host memory, runs
+  SolverPBF.step and copies particle_q / particle_qd back.
+* roofline: the dominant pass from the library's per-pass CUDA-event timer,
+  algorithmic bytes per particle per pass (constants below) / its average
+  launch time, against the measured HBM copy bandwidth.
+* cpu_baseline: the CPU oracle (C++ restatement of the reference solver,
+  OpenMP, all host threads) on a bounded number of substeps of the same
+  workload.  --impl reference times the same thing as the reference arm: the
+  reference (Warp + Newton) cannot be installed or run on these hosts.
+* Multi-GPU (torchrun): every rank advances its own replica (weak scaling, no
+  data-path collective); time = max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic HBM bytes per particle per pass launch (compulsory traffic under
+# the reference's pass dependencies: each per-particle array a pass uses is
+# read once, neighbour re-reads are cache hits, outputs written once; FP32,
+# vec3 = 12 B).  Per substep: PBF 728 B, WCSPH 180 B, DFSPH 328 B + 116 B per
+# density iteration + 108 B per divergence iteration.
+B_ALG = {
+    "grid_build": 48, "pbf_predict": 60, "pbf_density": 28, "pbf_accel": 72, "pbf_lambda": 40, "pbf_delta": 56,
+    "pbf_velocity": 44, "pbf_xsph": 64, "wcsph_density": 40, "wcsph_force": 92, "dfsph_density_factor": 36,
+    "dfsph_accel": 76, "dfsph_rate": 60, "dfsph_correct": 56, "dfsph_integrate": 36, "dfsph_final": 48,
+}
+PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 4090 (performance_summary.json)
+FALLBACK_HBM_GBS = 6650.0
+SUBSTEP_DT = {"pbf": 1.0 / 240.0, "dfsph": 1.0 / 240.0}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------- workloads ----
+def build_workload(name, device):
+    """(model, solver, dt, n, description)."""
+    from fluid_simulation_b200.dam_break import material, solver_config
+    from fluid_simulation_b200.newton_shim import model_from_arrays
+    from fluid_simulation_b200.scene import make_scene, stress_lattice
+    from fluid_simulation_b200.solver import SolverDFSPH, SolverPBF, SolverWCSPH
+    if name in ("pbf_dam_401856", "dfsph_dam_401856"):
+        kind = name.split("_")[0]
+        s = make_scene(400000)
+        cls = {"pbf": SolverPBF, "dfsph": SolverDFSPH}[kind]
+        attrs = dict(material(kind, s), particle_mask=0)
+        m = model_from_arrays(s.positions, np.zeros_like(s.positions), s.mass, device=device, radius=s.radius,
+                              gravity=(s.spec.gravity,), attributes=attrs, solver_cls=cls)
+        solver = cls(m, solver_config(kind, s))
+        desc = dict(workload=name, particles=s.count, scene="make_scene(400000) dam break",
+                    solver=kind.upper(), dt=SUBSTEP_DT[kind])
+        if kind == "pbf":
+            desc.update(constraint_iterations=4, substeps_per_frame=4, artificial_pressure="off (harness scorr_k=0)",
+                        xsph_c=0.05)
+        else:
+            desc.update(max_rho_iterations=5, max_vel_iterations=12, warm_start=False)
+        return m, solver, SUBSTEP_DT[kind], s.count, desc
+    if name == "wcsph_stress_4m":
+        x, v, sp = stress_lattice(cells=128, box=1.6)   # BCC: 2 * 128^3 = 4,194,304 at d = 9.92 mm
+        m = model_from_arrays(x, v, 1000.0 * sp ** 3, device=device, radius=0.5 * sp,
+                              attributes=dict(rest_density=1000.0, surface_tension=0.0, viscosity=1e-6,
+                                              stiffness=2.5e5, exponent=7.0, particle_mask=0), solver_cls=SolverWCSPH)
+        solver = SolverWCSPH(m, SolverWCSPH.SphConfig(particle_radius=0.5 * sp, particle_length=sp,
+                                                      smoothing_length_coff=2.0, boundary_damping=0.0,
+                                                      bound_width=0.8, bound_height=0.8, bound_length=0.8))
+        c0 = (2.5e5 * 7.0 / 1000.0) ** 0.5
+        h = 2.0 * sp
+        dt = 0.25 * h / (c0 + float(np.linalg.norm(v, axis=1).max()))
+        return m, solver, dt, len(x), dict(workload=name, particles=len(x), scene="jittered BCC lattice 2 x 128^3 "
+                                           "filling [-0.8,0.8]^2 x [0,1.6] m, v ~ N(0, 0.2)", solver="WCSPH", dt=dt,
+                                           h=h, spacing=sp)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_oracle_setup(name):
+    """Oracle-form model/state/config of the same workload (numpy)."""
+    from fluid_simulation_b200.dam_break import material, solver_config
+    from fluid_simulation_b200.scene import make_scene
+    from dataclasses import asdict
+    kind = name.split("_")[0]
+    s = make_scene(400000)
+    n = s.count
+    mat = material(kind, s)
+    sph = {k: np.full(n, val, np.float32) for k, val in mat.items()}
+    sph["particle_mask"] = np.zeros(n, np.int32)
+    model = dict(particle_flags=np.ones(n, np.int32), particle_mass=np.full(n, s.mass, np.float32),
+                 particle_world=np.zeros(n, np.int32), gravity=np.array([s.spec.gravity], np.float32),
+                 particle_max_radius=s.radius, sph=sph)
+    state = dict(particle_q=s.positions.copy(), particle_qd=np.zeros_like(s.positions), sph={})
+    return kind, model, state, asdict(solver_config(kind, s)), n
+
+
+def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1):
+    """Substeps of the CPU oracle until max_seconds have passed."""
+    import oracle
+    kind, model, state, cfg, n = cpu_oracle_setup(name)
+    step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step}[kind]
+    dt = SUBSTEP_DT[kind]
+    cores = oracle.num_threads(os.cpu_count() or 1)
+    k = 0
+    t0 = time.perf_counter()
+    while k < max_steps and (k < min_steps or time.perf_counter() - t0 < max_seconds):
+        out = step(model, state, cfg, dt)[0]
+        state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+        k += 1
+    el = time.perf_counter() - t0
+    return dict(value=n * k / el, unit="particle-steps/s", cores=cores, kind="port",
+                sample=f"{k} consecutive substeps of the full {n}-particle workload in {el:.1f} s "
+                       f"(C++ restatement of the reference solver, OpenMP, {cores} threads)")
+
+
+# --------------------------------------------------------------- clocks ----
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return dict(sm_mhz=statistics.median(sm), sm_max_mhz=mx, reasons=sorted(reasons), samples=len(sm))
+
+
+# ------------------------------------------------------------- our arm ----
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import ctypes as C
+    from fluid_simulation_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    lib = _lib.load()
+
+    model, solver, dt, n, desc = build_workload(args.workload, dev)
+    ctx = model.particle_grid._ctx
+    a, b = model.state(), model.state()
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        nonlocal a, b
+        solver.step(a, b, None, None, dt)
+        a, b = b, a
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    npass = lib.fs_pass_count()
+    _lib.check(lib.fs_timer_enable(ctx, max(64, 40 * K)), "timer")
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = lib.fs_launch_count(ctx)
+    for k in range(K):
+        ev[k][0].record()
+        step()
+        ev[k][1].record()
+        flush.zero_()
+    torch.cuda.synchronize()
+    launches = lib.fs_launch_count(ctx) - launches0
+    clk = clocks.stop()
+    ms = (C.c_float * npass)()
+    cnt = (C.c_int32 * npass)()
+    dropped = C.c_int32(0)
+    _lib.check(lib.fs_timer_read(ctx, ms, cnt, npass, C.byref(dropped)), "timer read")
+    step_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    t_local = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    total_ms = float(t_local.item())
+    value = world * n * K / (total_ms * 1e-3)
+
+    passes = {}
+    for p in range(npass):
+        if cnt[p]:
+            name = lib.fs_pass_name(p).decode()
+            passes[name] = dict(ms_total=round(ms[p], 4), launches=int(cnt[p]), ms_avg=round(ms[p] / cnt[p], 5))
+    dom = max(passes, key=lambda k: passes[k]["ms_total"])
+    peak, peak_kind = measured_peak()
+    bpl = B_ALG.get(dom, 0) * n
+    achieved = bpl / (passes[dom]["ms_avg"] * 1e-3) / 1e9
+    roofline = dict(bound="hbm", kernel=dom, achieved=round(achieved, 1), peak=peak, unit="GB/s",
+                    frac=round(achieved / peak, 4), peak_source=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    traffic=None, bytes_per_launch=bpl,
+                    share_of_step=round(passes[dom]["ms_total"] / max(step_ms, 1e-9), 3))
+    all_passes_b = sum(B_ALG.get(k, 0) * n * v["launches"] for k, v in passes.items())
+    step_roofline = dict(algorithmic_bytes_per_step=all_passes_b / K, achieved_gbs=round(
+        all_passes_b / (step_ms * 1e-3) / 1e9, 1), frac=round(all_passes_b / (step_ms * 1e-3) / 1e9 / peak, 4))
+
+    # ---- e2e through the solver API with host state
+    Ke = max(3, min(K, args.e2e_steps))
+    hx = a.particle_q.cpu().pin_memory()     # continue from the state the timed loop reached
+    hv = a.particle_qd.cpu().pin_memory()
+    ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(Ke)]
+    s_in, s_out = model.state(), model.state()
+    for k in range(Ke):
+        ee[k][0].record()
+        s_in.particle_q.copy_(hx, non_blocking=True)
+        s_in.particle_qd.copy_(hv, non_blocking=True)
+        solver.step(s_in, s_out, None, None, dt)
+        hx.copy_(s_out.particle_q, non_blocking=True)
+        hv.copy_(s_out.particle_qd, non_blocking=True)
+        ee[k][1].record()
+        flush.zero_()
+    torch.cuda.synchronize()
+    e2e_ms = sum(e0.elapsed_time(e1) for e0, e1 in ee)
+    t_e2e = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * Ke / (float(t_e2e.item()) * 1e-3)
+
+    # ---- secondary workloads (same timing rules, fewer steps), N=1 only
+    secondary = {}
+    if world == 1 and not args.no_secondary:
+        for wl in ("dfsph_dam_401856", "wcsph_stress_4m"):
+            if wl == args.workload:
+                continue
+            m2, s2, dt2, n2, d2 = build_workload(wl, dev)
+            x0, x1 = m2.state(), m2.state()
+            for _ in range(3):
+                s2.step(x0, x1, None, None, dt2)
+                x0, x1 = x1, x0
+            torch.cuda.synchronize()
+            k2 = max(5, min(30, K))
+            tot = 0.0
+            for _ in range(k2):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                s2.step(x0, x1, None, None, dt2)
+                e1.record()
+                x0, x1 = x1, x0
+                flush.zero_()
+                e1.synchronize()
+                tot += e0.elapsed_time(e1)
+            rec = dict(d2, value=round(n2 * k2 / (tot * 1e-3), 1), unit="particle-steps/s",
+                       ms_per_step=round(tot / k2, 4), steps=k2)
+            if wl.startswith("dfsph"):
+                rec["iterations_last_step"] = s2.last_iterations()
+            secondary[wl] = rec
+            del m2, s2, x0, x1
+            torch.cuda.empty_cache()
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline and args.workload != "wcsph_stress_4m":
+        cpu = time_cpu_baseline(args.workload, max_seconds=args.cpu_seconds)
+
+    if rank == 0:
+        line = dict(
+            metric="particle-steps/s", value=round(value, 1), unit="particle-steps/s", n_gpus=world, steps=K,
+            warmup=args.warmup, ms_per_step=round(total_ms / K, 5), higher_is_better=True, scaling="weak",
+            vs_baseline=round(value / PUBLISHED_PBF, 3) if args.workload == "pbf_dam_401856" else None,
+            dtype="f32", data="synthetic (reference dam-break scene generator, seeded)",
+            config=dict(desc, l2="flushed between timed steps (512 MB write outside the events)",
+                        parallelism="replicas" if world > 1 else "single GPU",
+                        grid="HashGrid(128,128,128), cell = h, truncating cell coordinates"),
+            e2e=dict(value=round(e2e_value, 1), unit="particle-steps/s", h2d_bytes_per_step=2 * n * 12,
+                     d2h_bytes_per_step=2 * n * 12, steps=Ke,
+                     path="host particle_q/qd (pinned) -> SolverPBF.step -> host"),
+            gpu_launches=int(launches), roofline=roofline, step_roofline=step_roofline, passes=passes,
+            timer_dropped=int(dropped.value), clocks=clk, cpu_baseline=cpu, secondary=secondary or None,
+        )
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if args.workload == "wcsph_stress_4m":
+        raise SystemExit("the reference arm covers the dam-break workloads")
+    kind, model, state, cfg, n = cpu_oracle_setup(args.workload)
+    import oracle
+    cores = oracle.num_threads(os.cpu_count() or 1)
+    step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step}[kind]
+    dt = SUBSTEP_DT[kind]
+    for _ in range(min(args.warmup, 1)):
+        out = step(model, state, cfg, dt)[0]
+        state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+    k = 0
+    t0 = time.perf_counter()
+    while k < args.steps and (k == 0 or time.perf_counter() - t0 < args.cpu_seconds * 3):
+        out = step(model, state, cfg, dt)[0]
+        state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+        k += 1
+    el = time.perf_counter() - t0
+    value = n * k / el
+    sample = (f"{k} of the requested {args.steps} substeps of the full {n}-particle workload in {el:.1f} s, "
+              f"C++ restatement of the reference solver (the reference needs warp-lang + newton, not "
+              f"installable here), OpenMP {cores} threads")
+    print(json.dumps(dict(
+        impl="reference", metric="particle-steps/s", value=round(value, 1), unit="particle-steps/s", n_gpus=0,
+        steps=k, warmup=min(args.warmup, 1), ms_per_step=round(el / k * 1e3, 3), higher_is_better=True,
+        scaling="weak", vs_baseline=None, dtype="f32", data="synthetic (reference dam-break scene generator)",
+        config=dict(workload=args.workload, particles=n, dt=dt),
+        cpu_baseline=dict(value=round(value, 1), unit="particle-steps/s", cores=cores, kind="port", sample=sample),
+        e2e=dict(value=round(value, 1), unit="particle-steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+    )), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pbf_dam_401856",
+                    choices=["pbf_dam_401856", "dfsph_dam_401856", "wcsph_stress_4m"])
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

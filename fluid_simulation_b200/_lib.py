@@ -99,6 +99,13 @@ SIGNATURES = {
     "fs_pbf_lambda": (C.c_int, [P, C.POINTER(Model), P, C.POINTER(PbfParams), P, P, P, P]),
     "fs_pbf_delta": (C.c_int, [P, C.POINTER(Model), P, P, C.POINTER(PbfParams), P, P]),
     "fs_pbf_xsph": (C.c_int, [P, C.POINTER(Model), P, P, P, F, F, P, P]),
+    "fs_norm_maxima": (C.c_int, [P, I64, P, I64, P, P]),
+    "fs_check_finite": (C.c_int, [P, P, I64, P, I64, P, P]),
+    "fs_pass_count": (I32, []),
+    "fs_pass_name": (C.c_char_p, [I32]),
+    "fs_timer_enable": (C.c_int, [P, I32]),
+    "fs_timer_read": (C.c_int, [P, P, P, I32, P]),
+    "fs_launch_count": (I64, [P]),
     "fs_status_read": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "fs_status_clear": (C.c_int, [P, P]),
     "fs_last_error_string": (C.c_char_p, []),

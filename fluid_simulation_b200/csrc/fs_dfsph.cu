@@ -402,7 +402,10 @@ int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float 
   a.ctrl = ctrl;
   a.red_part = c->red_part;
   a.red_cnt = c->red_cnt;
-  k_rate<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  {
+    PassScope ps_(c, P_DFSPH_RATE, st);
+    k_rate<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  }
   return launch_check("dfsph rate");
 }
 
@@ -420,7 +423,10 @@ int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float
   a.kappa_api = kappa_api;
   a.vstar_api = vstar_api;
   a.ctrl = ctrl;
-  k_correct<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  {
+    PassScope ps_(c, P_DFSPH_CORRECT, st);
+    k_correct<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  }
   return launch_check("dfsph correct");
 }
 
@@ -438,7 +444,10 @@ int run_density_factor(fs_context* c, const fs_model* m, float h, int min_nb, fl
   a.factor = factor;
   a.count = count;
   a.sc2 = c->sc2;
-  k_density_factor<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  {
+    PassScope ps_(c, P_DFSPH_DENSITY_FACTOR, st);
+    k_density_factor<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  }
   return launch_check("dfsph density/factor");
 }
 
@@ -470,8 +479,11 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   if ((rc = check_cuda(cudaMemsetAsync(c->dfsph, 0, sizeof(DfsphDev) * 2, st), "dfsph reset"))) return rc;
   // ---- first half: positions x_in
   if ((rc = grid_build(c, si->particle_q, n, h, st))) return rc;
-  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, si->particle_q, si->particle_qd, c->xs, c->vs,
+  {
+    PassScope ps_(c, P_GATHER, st);
+    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, si->particle_q, si->particle_qd, c->xs, c->vs,
                                                     c->mv, c->status);
+  }
   {
     // density/factor reads masses from vs2.w: fill it from vs (v_in, mass) first
     if ((rc = check_cuda(cudaMemcpyAsync(c->vs2, c->vs, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st),
@@ -492,10 +504,16 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   aa.dt = dt;
   aa.accel = accel;
   aa.vstar = c->vs2;
-  k_accel_predict<<<blocks_for(n), kBlock, 0, st>>>(aa);
+  {
+    PassScope ps_(c, P_DFSPH_ACCEL, st);
+    k_accel_predict<<<blocks_for(n), kBlock, 0, st>>>(aa);
+  }
   if ((rc = launch_check("dfsph accel"))) return rc;
   if (p->warm_start) {
-    k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa, c->sc1, nullptr);
+    {
+      PassScope ps_(c, P_GATHER, st);
+      k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa, c->sc1, nullptr);
+    }
     if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa, nullptr, nullptr, st))) return rc;
   }
   for (int it = 0; it < p->max_rho_iterations; ++it) {
@@ -504,16 +522,25 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
       return rc;
     if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa, nullptr, c->dfsph + 0, st))) return rc;
   }
-  k_integrate<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, dt, so->particle_q, so->v_star);
+  {
+    PassScope ps_(c, P_DFSPH_INTEGRATE, st);
+    k_integrate<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, dt, so->particle_q, so->v_star);
+  }
   if ((rc = launch_check("dfsph integrate"))) return rc;
   // ---- second half: positions x_out
   if ((rc = grid_build(c, so->particle_q, n, h, st))) return rc;
-  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, so->particle_q, so->v_star, c->xs, c->vs2, c->mv,
+  {
+    PassScope ps_(c, P_GATHER, st);
+    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, so->particle_q, so->v_star, c->xs, c->vs2, c->mv,
                                                     c->status);
+  }
   if ((rc = run_density_factor(c, m, h, p->min_neighbors_for_factor, so->rho, so->factor, so->neighbor_count, st)))
     return rc;
   if (p->warm_start) {
-    k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa_v, c->sc1, nullptr);
+    {
+      PassScope ps_(c, P_GATHER, st);
+      k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa_v, c->sc1, nullptr);
+    }
     if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa_v, nullptr, nullptr, st))) return rc;
   }
   for (int it = 0; it < p->max_vel_iterations; ++it) {
@@ -523,7 +550,10 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
     if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa_v, nullptr, c->dfsph + 1, st))) return rc;
   }
   const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 1, 0.f, 0.f);
-  k_final<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, w, so->particle_q, so->particle_qd, so->v_star);
+  {
+    PassScope ps_(c, P_DFSPH_FINAL, st);
+    k_final<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, w, so->particle_q, so->particle_qd, so->v_star);
+  }
   c->last_stream = st;
   return launch_check("dfsph final");
 }
@@ -592,8 +622,11 @@ int fs_dfsph_residual(fs_context* c, const fs_model* m, const float* a, const fl
   const int64_t n = m->n > 0 ? m->n : 1;
   if (cudaMemsetAsync(c->dfsph, 0, sizeof(DfsphDev), st) != cudaSuccess)
     return set_error(FS_ERR_CUDA, "fs_dfsph_residual: memset");
-  k_residual<<<blocks_for(n), kBlock, 0, st>>>(m->n, m->particle_flags, m->particle_mask, a, b, c->red_part,
+  {
+    PassScope ps_(c, P_OTHER, st);
+    k_residual<<<blocks_for(n), kBlock, 0, st>>>(m->n, m->particle_flags, m->particle_mask, a, b, c->red_part,
                                                c->red_cnt, c->dfsph, out);
+  }
   return launch_check("fs_dfsph_residual");
 }
 

@@ -204,6 +204,7 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
   if (n > c->capacity) return set_error(FS_ERR_CAPACITY, "grid_build: n=%lld > capacity=%lld", (long long)n,
                                         (long long)c->capacity);
   const float inv = 1.0f / radius;
+  PassScope ps_(c, P_GRID, st, n > 0 ? 6 : 3);
   int rc = check_cuda(cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * c->ncell, st), "memset cell counts");
   if (rc) return rc;
   if (n > 0)
@@ -305,9 +306,12 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
   return FS_OK;
 }
 
+static void timer_free(PassTimer& t);
+
 int fs_context_destroy(fs_context* c) {
   if (!c) return FS_OK;
   DeviceGuard dg(c->device);
+  timer_free(c->timer);
   void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->scan_part, c->xs, c->xs2,
                 c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
                 c->dfsph, c->status};
@@ -331,8 +335,11 @@ int fs_grid_tables(fs_context* c, int32_t* point_ids, int32_t* point_cells, int3
   if (c->built_n < 0) return set_error(FS_ERR_NOGRID, "fs_grid_tables: no grid built");
   DeviceGuard dg(c->device);
   const int64_t m = c->built_n > c->ncell ? c->built_n : c->ncell;
-  k_tables<<<blocks_for(m), kBlock, 0, (cudaStream_t)stream>>>(c->built_n, c->ncell, c->perm, c->key, c->cell_off,
+  {
+    PassScope ps_(c, P_OTHER, (cudaStream_t)stream);
+    k_tables<<<blocks_for(m), kBlock, 0, (cudaStream_t)stream>>>(c->built_n, c->ncell, c->perm, c->key, c->cell_off,
                                                                point_ids, point_cells, cell_starts, cell_ends);
+  }
   return launch_check("fs_grid_tables");
 }
 
@@ -345,11 +352,88 @@ int fs_grid_candidates(fs_context* c, const float* q, int64_t nq, float r, int64
   DeviceGuard dg(c->device);
   GridDev g = grid_view(c);
   cudaStream_t st = (cudaStream_t)stream;
-  if (cand)
+  if (cand) {
+    PassScope ps_(c, P_OTHER, st);
     k_candidates<true><<<blocks_for(nq), kBlock, 0, st>>>(g, q, nq, r, counts, offsets, cand);
+  }
   else
-    k_candidates<false><<<blocks_for(nq), kBlock, 0, st>>>(g, q, nq, r, counts, nullptr, nullptr);
+    {
+      PassScope ps_(c, P_OTHER, st);
+      k_candidates<false><<<blocks_for(nq), kBlock, 0, st>>>(g, q, nq, r, counts, nullptr, nullptr);
+    }
   return launch_check("fs_grid_candidates");
+}
+
+static const char* kPassNames[P_COUNT] = {
+    "grid_build", "gather", "wcsph_density", "wcsph_force", "dfsph_density_factor", "dfsph_accel", "dfsph_rate",
+    "dfsph_correct", "dfsph_integrate", "dfsph_final", "pbf_predict", "pbf_density", "pbf_accel", "pbf_lambda",
+    "pbf_delta", "pbf_velocity", "pbf_xsph", "other"};
+
+int32_t fs_pass_count(void) { return P_COUNT; }
+
+const char* fs_pass_name(int32_t pass) { return (pass >= 0 && pass < P_COUNT) ? kPassNames[pass] : ""; }
+
+int64_t fs_launch_count(const fs_context* c) { return c ? c->launches : -1; }
+
+static void timer_free(PassTimer& t) {
+  if (t.ev) {
+    for (int k = 0; k < 2 * t.cap; ++k) cudaEventDestroy(t.ev[k]);
+    delete[] t.ev;
+    delete[] t.pass_of;
+  }
+  t = PassTimer{};
+}
+
+int fs_timer_enable(fs_context* c, int32_t capacity) {
+  if (!c || capacity < 0) return set_error(FS_ERR_INVALID, "fs_timer_enable: bad arguments");
+  DeviceGuard dg(c->device);
+  PassTimer& t = c->timer;
+  if (capacity == 0) {
+    timer_free(t);
+    return FS_OK;
+  }
+  if (t.cap != capacity) {
+    timer_free(t);
+    t.ev = new cudaEvent_t[2 * (size_t)capacity];
+    t.pass_of = new int[capacity];
+    for (int k = 0; k < 2 * capacity; ++k) {
+      int rc = check_cuda(cudaEventCreate(&t.ev[k]), "fs_timer_enable: cudaEventCreate");
+      if (rc) {
+        t.cap = k / 2;
+        timer_free(t);
+        return rc;
+      }
+    }
+    t.cap = capacity;
+  }
+  t.used = 0;
+  t.dropped = 0;
+  t.on = true;
+  return FS_OK;
+}
+
+int fs_timer_read(fs_context* c, float* ms_per_pass, int32_t* launches_per_pass, int32_t npass, int32_t* dropped) {
+  if (!c || !ms_per_pass || !launches_per_pass || npass < P_COUNT)
+    return set_error(FS_ERR_INVALID, "fs_timer_read: bad arguments");
+  DeviceGuard dg(c->device);
+  PassTimer& t = c->timer;
+  for (int p = 0; p < npass; ++p) {
+    ms_per_pass[p] = 0.f;
+    launches_per_pass[p] = 0;
+  }
+  for (int k = 0; k < t.used; ++k) {
+    int rc = check_cuda(cudaEventSynchronize(t.ev[2 * k + 1]), "fs_timer_read: sync");
+    if (rc) return rc;
+    float ms = 0.f;
+    rc = check_cuda(cudaEventElapsedTime(&ms, t.ev[2 * k], t.ev[2 * k + 1]), "fs_timer_read: elapsed");
+    if (rc) return rc;
+    ms_per_pass[t.pass_of[k]] += ms;
+    launches_per_pass[t.pass_of[k]] += 1;
+  }
+  if (dropped) *dropped = t.dropped;
+  t.on = false;
+  t.used = 0;
+  return FS_OK;
 }
 
 int fs_status_read(fs_context* c, uint32_t* status) {

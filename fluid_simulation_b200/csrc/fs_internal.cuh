@@ -28,6 +28,20 @@ struct DfsphDev {     // device-resident per-step DFSPH control block
   double residual;    // last residual of this half
 };
 
+// Passes for the per-pass CUDA-event timer (fs_timer_*) and launch counter.
+enum Pass {
+  P_GRID = 0, P_GATHER, P_WCSPH_DENSITY, P_WCSPH_FORCE, P_DFSPH_DENSITY_FACTOR, P_DFSPH_ACCEL, P_DFSPH_RATE,
+  P_DFSPH_CORRECT, P_DFSPH_INTEGRATE, P_DFSPH_FINAL, P_PBF_PREDICT, P_PBF_DENSITY, P_PBF_ACCEL, P_PBF_LAMBDA,
+  P_PBF_DELTA, P_PBF_VELOCITY, P_PBF_XSPH, P_OTHER, P_COUNT
+};
+
+struct PassTimer {
+  bool on = false;
+  int cap = 0, used = 0, dropped = 0;
+  cudaEvent_t* ev = nullptr;  // 2 * cap events
+  int* pass_of = nullptr;     // pass of each recorded pair
+};
+
 struct GridDev {
   const int32_t* off;   // [ncell + 1] exclusive prefix of cell occupancy (hash-key order)
   const int32_t* perm;  // [n] sorted slot -> original particle index (warp's point_ids)
@@ -72,6 +86,10 @@ struct fs_context {
   int64_t* red_cnt = nullptr;   // [reduction blocks]
   fs::DfsphDev* dfsph = nullptr; // [2] control blocks (density half, divergence half)
   uint32_t* status = nullptr;
+
+  // instrumentation
+  fs::PassTimer timer;
+  int64_t launches = 0;  // kernels launched through this context (host count)
 };
 
 namespace fs {
@@ -95,6 +113,29 @@ struct DeviceGuard {
 };
 
 inline int blocks_for(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+// Brackets the launches of one pass: counts them and, when the timer is on,
+// records a CUDA event pair around them on the launching stream.
+struct PassScope {
+  fs_context* c;
+  cudaStream_t st;
+  int slot = -1;
+  PassScope(fs_context* ctx, int pass, cudaStream_t stream, int nkernels = 1) : c(ctx), st(stream) {
+    c->launches += nkernels;
+    PassTimer& t = c->timer;
+    if (!t.on) return;
+    if (t.used >= t.cap) {
+      ++t.dropped;
+      return;
+    }
+    slot = t.used++;
+    t.pass_of[slot] = pass;
+    cudaEventRecord(t.ev[2 * slot], st);
+  }
+  ~PassScope() {
+    if (slot >= 0) cudaEventRecord(c->timer.ev[2 * slot + 1], st);
+  }
+};
 
 // grid build (fs_grid.cu)
 int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st);

@@ -339,9 +339,15 @@ __global__ void k_scalar_to_pair(int64_t n, const float* __restrict__ a, float2*
 
 int gather_pbf(fs_context* c, const fs_model* m, const float* x_in, cudaStream_t st) {
   const int64_t n = m->n;
-  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, c->xo_tmp, c->vo_tmp, c->xs, c->vs, c->mv,
+  {
+    PassScope ps_(c, P_GATHER, st);
+    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, c->xo_tmp, c->vo_tmp, c->xs, c->vs, c->mv,
                                                     c->status);
-  k_gather_xin<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, x_in, c->vs2);
+  }
+  {
+    PassScope ps_(c, P_GATHER, st);
+    k_gather_xin<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, x_in, c->vs2);
+  }
   return launch_check("pbf gather");
 }
 
@@ -370,12 +376,18 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 2,
                              p->particle_radius, p->boundary_epsilon);
   int rc;
-  k_predict<<<blocks_for(n), kBlock, 0, st>>>(n, *m, si->particle_q, si->particle_qd, dt, w, c->xo_tmp, c->vo_tmp);
+  {
+    PassScope ps_(c, P_PBF_PREDICT, st);
+    k_predict<<<blocks_for(n), kBlock, 0, st>>>(n, *m, si->particle_q, si->particle_qd, dt, w, c->xo_tmp, c->vo_tmp);
+  }
   if ((rc = launch_check("pbf predict"))) return rc;
   if ((rc = grid_build(c, c->xo_tmp, n, h, st))) return rc;
   if ((rc = gather_pbf(c, m, si->particle_q, st))) return rc;
   const GridDev g = grid_view(c);
-  k_density<<<blocks_for(n), kBlock, 0, st>>>(g, n, c->xs, c->mv, h, so->rho, c->sc2);
+  {
+    PassScope ps_(c, P_PBF_DENSITY, st);
+    k_density<<<blocks_for(n), kBlock, 0, st>>>(g, n, c->xs, c->mv, h, so->rho, c->sc2);
+  }
   AccelArgs aa;
   aa.g = g;
   aa.n = n;
@@ -389,7 +401,10 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   aa.walls = w;
   aa.accel = accel;
   aa.xs_out = c->xs2;
-  k_accel_apply<<<blocks_for(n), kBlock, 0, st>>>(aa);
+  {
+    PassScope ps_(c, P_PBF_ACCEL, st);
+    k_accel_apply<<<blocks_for(n), kBlock, 0, st>>>(aa);
+  }
   if ((rc = launch_check("pbf accel"))) return rc;
   float4* cur = c->xs2;
   float4* nxt = c->xs;
@@ -408,7 +423,10 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     la.lam = so->pbf_lambda;
     la.rho = so->rho;
     la.count = so->neighbor_count;
-    k_lambda<<<blocks_for(n), kBlock, 0, st>>>(la);
+    {
+      PassScope ps_(c, P_PBF_LAMBDA, st);
+      k_lambda<<<blocks_for(n), kBlock, 0, st>>>(la);
+    }
     DeltaArgs da;
     da.g = gi;
     da.n = n;
@@ -425,14 +443,20 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     da.walls = w;
     da.delta_p = so->delta_p;
     da.xs_out = nxt;
-    k_delta<<<blocks_for(n), kBlock, 0, st>>>(da);
+    {
+      PassScope ps_(c, P_PBF_DELTA, st);
+      k_delta<<<blocks_for(n), kBlock, 0, st>>>(da);
+    }
     if ((rc = launch_check("pbf iteration"))) return rc;
     float4* t = cur;
     cur = nxt;
     nxt = t;
     if (p->rebuild_grid_each_iteration) {
       // x_pred back to original order, rebuild, regather (v_pred/x_in follow)
-      k_scatter_x<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, cur, c->xo_tmp);
+      {
+        PassScope ps_(c, P_GATHER, st);
+        k_scatter_x<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, cur, c->xo_tmp);
+      }
       if ((rc = grid_build(c, c->xo_tmp, n, h, st))) return rc;
       if ((rc = gather_pbf(c, m, si->particle_q, st))) return rc;
       cur = c->xs;
@@ -441,8 +465,14 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   }
   // final density on the bounded x_pred (bounds were fused into the last apply)
   const GridDev gf = grid_view(c);
-  k_density<<<blocks_for(n), kBlock, 0, st>>>(gf, n, cur, c->mv, h, so->rho, c->sc2);
-  k_velocity<<<blocks_for(n), kBlock, 0, st>>>(n, cur, c->vs2, c->vs, dt, nxt);
+  {
+    PassScope ps_(c, P_PBF_DENSITY, st);
+    k_density<<<blocks_for(n), kBlock, 0, st>>>(gf, n, cur, c->mv, h, so->rho, c->sc2);
+  }
+  {
+    PassScope ps_(c, P_PBF_VELOCITY, st);
+    k_velocity<<<blocks_for(n), kBlock, 0, st>>>(n, cur, c->vs2, c->vs, dt, nxt);
+  }
   XsphArgs xa;
   xa.g = gf;
   xa.n = n;
@@ -456,7 +486,10 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   xa.x_out = so->particle_q;
   xa.v_out = so->particle_qd;
   xa.x_pred_api = x_pred;
-  k_xsph_final<<<blocks_for(n), kBlock, 0, st>>>(xa);
+  {
+    PassScope ps_(c, P_PBF_XSPH, st);
+    k_xsph_final<<<blocks_for(n), kBlock, 0, st>>>(xa);
+  }
   c->last_stream = st;
   return launch_check("pbf final");
 }

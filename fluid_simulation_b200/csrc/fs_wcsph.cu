@@ -173,7 +173,10 @@ __global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const
 
 int wcsph_gather(fs_context* c, const fs_model* m, const float* x, const float* v, cudaStream_t st) {
   const int64_t n = m->n;
-  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, x, v, c->xs, c->vs, c->mv, c->status);
+  {
+    PassScope ps_(c, P_GATHER, st);
+    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, x, v, c->xs, c->vs, c->mv, c->status);
+  }
   return launch_check("wcsph gather");
 }
 
@@ -192,7 +195,10 @@ int launch_density(fs_context* c, const fs_model* m, float h, int clamp, bool eo
   a.rho = rho;
   a.pressure = pressure;
   a.sc2 = c->sc2;
-  k_wcsph_density<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  {
+    PassScope ps_(c, P_WCSPH_DENSITY, st);
+    k_wcsph_density<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  }
   return launch_check("wcsph density");
 }
 
@@ -212,7 +218,10 @@ int launch_force(fs_context* c, const fs_model* m, const fs_wcsph_params* p, flo
   a.accel = accel;
   a.x_out = x_out;
   a.v_out = v_out;
-  k_wcsph_force<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  {
+    PassScope ps_(c, P_WCSPH_FORCE, st);
+    k_wcsph_force<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+  }
   return launch_check("wcsph force");
 }
 

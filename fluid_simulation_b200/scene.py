@@ -116,14 +116,21 @@ def jittered_column(target=10000, seed=0, lo=(-1.2, -0.28, 0.0), hi=(-0.6, 0.28,
     return x.astype(np.float32), spacing
 
 
-def stress_lattice(side=128, spacing=0.0125, seed_x=0, seed_v=1, sigma_v=0.2, jitter=0.01):
-    """side^3 jittered lattice filling [-side*dx/2, side*dx/2]^2 x [0, side*dx]
-    (128^3 at dx = 0.0125 m fills [-0.8,0.8]^2 x [0,1.6]); v ~ N(0, sigma_v)."""
-    c = (np.arange(side, dtype=np.float64) + 0.5) * spacing
-    xs = c - 0.5 * side * spacing
-    zs = c
-    g = np.meshgrid(xs, xs, zs, indexing="ij")
-    x = np.stack([a.ravel() for a in g], 1)
-    x += np.random.default_rng(seed_x).uniform(-jitter, jitter, x.shape) * spacing
+def stress_lattice(cells=128, box=1.6, seed_x=0, seed_v=1, sigma_v=0.2, jitter=0.01, bcc=True):
+    """Neighbour-search stress input: a jittered cubic lattice filling the
+    box [-box/2, box/2]^2 x [0, box].  With ``bcc`` (default) every cubic cell
+    of side a = box / cells holds a corner and a body-centre particle, so
+    2 * 128^3 = 4,194,304 particles fill a 1.6 m cube at the rest spacing
+    d = a / 2^(1/3) (9.92 mm; h = 2 d gives ~33 neighbours).  Jitter is
+    U(-jitter, jitter) x d (default_rng(seed_x)); v ~ N(0, sigma_v) per
+    component (default_rng(seed_v)).  Returns (x, v, d)."""
+    a = box / cells
+    c = (np.arange(cells, dtype=np.float64) + 0.25) * a
+    g = np.meshgrid(c - 0.5 * box, c - 0.5 * box, c, indexing="ij")
+    x = np.stack([t.ravel() for t in g], 1)
+    if bcc:
+        x = np.concatenate([x, x + 0.5 * a], 0)
+    d = a / (2.0 ** (1.0 / 3.0)) if bcc else a
+    x += np.random.default_rng(seed_x).uniform(-jitter, jitter, x.shape) * d
     v = np.random.default_rng(seed_v).normal(0.0, sigma_v, x.shape)
-    return x.astype(np.float32), v.astype(np.float32)
+    return x.astype(np.float32), v.astype(np.float32), d

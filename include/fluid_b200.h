@@ -200,6 +200,28 @@ int fs_pbf_delta(fs_context* ctx, const fs_model* model, const float* x_pred, co
 int fs_pbf_xsph(fs_context* ctx, const fs_model* model, const float* x_pred, const float* v_in, const float* rho,
                 float h, float xsph_c, float* v_out, fs_stream_t stream);
 
+/* ---- dam-break harness reductions (examples/dam_break/simulation.py) -----
+ * particle_norm_maxima (19-36): out[0] = max |v|^2 over nv rows, out[1] =
+ * max |a|^2 over na rows (a non-finite vector counts as +inf); out is a
+ * device float[2] and is zeroed by the call. */
+int fs_norm_maxima(const float* v, int64_t nv, const float* a, int64_t na, float* out, fs_stream_t stream);
+/* check_particle_finite (39-53): *invalid (device int32) = 1 if any of x[n],
+ * v[n], rho[nrho] is non-finite, else 0. */
+int fs_check_finite(const float* x, const float* v, int64_t n, const float* rho, int64_t nrho, int32_t* invalid,
+                    fs_stream_t stream);
+
+/* ---- instrumentation (no counterpart in the reference, which only times
+ * whole frames with wall clocks: examples/dam_break/benchmark.py:63-72) ----
+ * Per-pass CUDA-event timer: while enabled, every pass launched through the
+ * context is bracketed by an event pair on its stream (up to `capacity`
+ * passes).  fs_timer_read synchronises, sums the elapsed time per pass id
+ * (names from fs_pass_name) and disables the timer. */
+int32_t fs_pass_count(void);
+const char* fs_pass_name(int32_t pass);
+int fs_timer_enable(fs_context* ctx, int32_t capacity); /* capacity 0 frees the events */
+int fs_timer_read(fs_context* ctx, float* ms_per_pass, int32_t* launches_per_pass, int32_t npass, int32_t* dropped);
+int64_t fs_launch_count(const fs_context* ctx);           /* kernels launched through ctx so far */
+
 /* ---- status ------------------------------------------------------------ */
 int fs_status_read(fs_context* ctx, uint32_t* status); /* synchronises the context's last stream */
 int fs_status_clear(fs_context* ctx, fs_stream_t stream);

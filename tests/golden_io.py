@@ -60,3 +60,12 @@ def velocity_scale(v_ref, x_ref, dt, tol):
     vmax = float(np.abs(v_ref).max())
     xmax = float(np.abs(x_ref).max())
     return max(vmax, 4.0 * float(np.finfo(np.float32).eps) * xmax / (dt * tol))
+
+
+# PBF lambda = -max(rho/rho0 - 1, 0) / (sum |grad C|^2 + eps) subtracts two O(1)
+# numbers: a density agreeing to FP32 rounding (relative 1e-7..1e-6) moves C
+# by that much, i.e. by (rho/rho0) / C relative in lambda, ~1e2 at the dam's
+# 1 % compression.  Lambda and the Jacobi correction delta_p built from it
+# are therefore held to 1e-3 of their maximum, while the particle positions,
+# velocities and densities they produce stay within 1e-5.
+CONDITIONED_TOL = {"pbf_lambda": 1e-3, "delta_p": 1e-3}

@@ -23,8 +23,8 @@ def point_sets():
         (128, 128, 128), 0
     yield "negative_floor", rng.uniform(-0.5, 0.5, (8000, 3)).astype(np.float32), 0.05, (128, 128, 128), 1
     yield "small_dims", rng.uniform(-0.3, 0.7, (5000, 3)).astype(np.float32), 0.04, (7, 5, 3), 0
-    x, _ = stress_lattice(side=24, spacing=0.0125)
-    yield "lattice24", x, 0.025, (128, 128, 128), 0
+    x, _, sp = stress_lattice(cells=20, box=0.25)
+    yield "bcc_lattice", x, 2.0 * sp, (128, 128, 128), 0
     yield "single_cell", np.full((37, 3), 0.01, np.float32), 0.1, (128, 128, 128), 0
 
 
