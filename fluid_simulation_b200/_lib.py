@@ -106,6 +106,7 @@ SIGNATURES = {
     "fs_timer_enable": (C.c_int, [P, I32]),
     "fs_timer_read": (C.c_int, [P, P, P, I32, P]),
     "fs_launch_count": (I64, [P]),
+    "fs_list_stats": (C.c_int, [P, P, I32, I32]),
     "fs_status_read": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "fs_status_clear": (C.c_int, [P, P]),
     "fs_last_error_string": (C.c_char_p, []),

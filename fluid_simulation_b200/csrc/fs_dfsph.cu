@@ -10,11 +10,14 @@
 // Launches of iterations after the break see `done` and return at once, so
 // the whole step is launch-only (graph capturable) and takes exactly the
 // reference's decisions.
-#include "fs_internal.cuh"
+#include "fs_nbr.cuh"
 
 namespace fs {
 
-int reduction_blocks(int64_t n) { return blocks_for(n > 0 ? n : 1); }
+// Partial-sum slots for the residual reductions: one per block of the
+// smallest block size that launches them (the 64-thread floor leaves room for
+// any block size used here).
+int reduction_blocks(int64_t n) { return blocks_for(n > 0 ? n : 1, 64); }
 
 // gathers of fs_wcsph.cu reused here
 __global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
@@ -38,6 +41,7 @@ __global__ void k_gather_scalar(int64_t n, const int32_t* __restrict__ perm, con
 // compute_density (107-133) + compute_factor_dfsph (137-174), one candidate loop.
 struct DensFactorArgs {
   GridDev g;
+  NbrList L;
   int64_t n;
   const float4* xs;
   const float4* vs;  // .w = mass
@@ -50,8 +54,11 @@ struct DensFactorArgs {
   float2* sc2;       // (rho, factor) cell order
 };
 
-__global__ void __launch_bounds__(kBlock) k_density_factor(DensFactorArgs a) {
+// Records the neighbour lists of this grid (positions stay fixed for the half
+// step, so every later pass of the half reuses them exactly).
+__global__ void __launch_bounds__(kNbBlock) k_density_factor(DensFactorArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  lists_recorded(a.L);
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
   const int32_t i = a.g.perm[s];
@@ -60,27 +67,25 @@ __global__ void __launch_bounds__(kBlock) k_density_factor(DensFactorArgs a) {
     a.factor[i] = 0.f;
     a.count[i] = 0;
     a.sc2[s] = make_float2(0.f, 0.f);
+    a.L.cnt[s] = 0;
     return;
   }
-  const CubicK K(a.h);
-  const float h2m = a.h * a.h * 1.000002f;
+  const float h2m = a.h * a.h * kSupportMargin;
+  // the candidate count (no distance test, solver_dfsph.py:163-164) comes from the scan
+  const int cnt = record_list<true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
+  const Cubic K(a.h);
   float rho = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sq = 0.f;
-  int cnt = 0;
-  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-    const float4 xj = __ldg(a.xs + t);
-    if (!(pf_of(xj) & PF_ACTIVE)) return;
-    cnt += (t != s) ? 1 : 0;  // candidates, no distance test (solver_dfsph.py:163-164)
+  visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = dist2_rn(dx, dy, dz);
-    if (r2 > h2m) return;
-    const float r = sqrtf(r2);
-    rho += __ldg(a.mv + t) * K.w(r);
-    const float gsc = __ldg(&a.vs[t].w) * K.dw_scale(r);
+    float r, rinv;
+    r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
+    rho = fmaf(__ldg(a.mv + t), K.w(r), rho);
+    const float gsc = __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
     const float gx = gsc * dx, gy = gsc * dy, gz = gsc * dz;
     sgx += gx;
     sgy += gy;
     sgz += gz;
-    sq += gx * gx + gy * gy + gz * gz;
+    sq = fmaf(gx, gx, fmaf(gy, gy, fmaf(gz, gz, sq)));
   });
   const float denom = (sgx * sgx + sgy * sgy + sgz * sgz) + sq;
   const float f = (cnt < a.min_nb || denom < 1.0e-6f) ? 0.f : 1.0f / denom;
@@ -93,6 +98,8 @@ __global__ void __launch_bounds__(kBlock) k_density_factor(DensFactorArgs a) {
 // acceleration_non_pressure (178-226) + predict_velocity (230-242).
 struct AccelArgs {
   GridDev g;
+  NbrList L;
+  int use_lists;
   int64_t n;
   const float4* xs;
   const float4* vs;
@@ -103,7 +110,7 @@ struct AccelArgs {
   float4* vstar;     // cell order (v*, mass)
 };
 
-__global__ void __launch_bounds__(kBlock) k_accel_predict(AccelArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_accel_predict(AccelArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
@@ -114,28 +121,28 @@ __global__ void __launch_bounds__(kBlock) k_accel_predict(AccelArgs a) {
     a.vstar[s] = make_float4(0.f, 0.f, 0.f, vi.w);
     return;
   }
-  const float mu = a.m.viscosity[i];
+  const float mu10 = 10.f * a.m.viscosity[i];
   const float coh = a.m.surface_tension[i] / vi.w;
   const float visc_den_add = 0.01f * (a.h * a.h);
-  const CubicK K(a.h);
-  const float h2m = a.h * a.h * 1.000002f;
+  const Cubic K(a.h);
   float ax = 0.f, ay = 0.f, az = 0.f;
-  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-    if (t == s) return;
-    const float4 xj = __ldg(a.xs + t);
+  const bool lists_ok = a.use_lists && lists_usable(a.L);
+  visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                      [&](int t, float4 xj) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = dist2_rn(dx, dy, dz);
-    if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (r2 == 0.f) return;  // zero vector d: every term vanishes
     const float4 vj = __ldg(a.vs + t);
     const float rho_j = __ldg(&a.sc2[t].x);
-    const float r = sqrtf(r2);
+    float r, rinv;
+    r_and_inv(r2, r, rinv);
     const float wc = coh * vj.w * K.w(fmaxf(r, a.particle_radius));
-    const float vdot = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
-    const float visc = 10.f * mu * (vj.w / fmaxf(rho_j, 1.0e-6f)) * vdot / (r * r + visc_den_add);
-    const float c = visc * K.dw_scale(r) - wc;
-    ax += c * dx;
-    ay += c * dy;
-    az += c * dz;
+    const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+    const float visc = mu10 * __fdividef(vj.w, fmaxf(rho_j, 1.0e-6f)) * __fdividef(vdot, r2 + visc_den_add);
+    const float c = fmaf(visc, K.grad_scale(r, rinv), -wc);
+    ax = fmaf(c, dx, ax);
+    ay = fmaf(c, dy, ay);
+    az = fmaf(c, dz, az);
   });
   const float3 g = gravity_of(a.m, i);
   const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
@@ -160,6 +167,9 @@ struct RateArgs {
   float* d_rho_dt;          // API
   float* rho_star;          // API (mode 0)
   float* kappa_new;         // cell order candidate kappa
+  float* kratio_new;        // cell order kappa / max(rho, 1e-6) (the correction's per-particle term)
+  NbrList L;
+  int use_lists;
   DfsphDev* ctrl;           // null: separate-pass use, no residual
   double* red_part;
   int64_t* red_cnt;
@@ -235,7 +245,7 @@ __device__ bool last_block(uint32_t* ticket) {
   return am_last;
 }
 
-__global__ void __launch_bounds__(kBlock) k_rate(RateArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_rate(RateArgs a) {
   if (a.ctrl && a.ctrl->done) return;  // uniform across the grid: set by an earlier launch
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double term = 0.0;
@@ -247,17 +257,16 @@ __global__ void __launch_bounds__(kBlock) k_rate(RateArgs a) {
     float d = 0.f;
     if (pf & PF_ACTIVE) {
       const float4 vi = a.vstar[s];
-      const CubicK K(a.h);
-      const float h2m = a.h * a.h * 1.000002f;
-      for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-        if (t == s) return;  // zero gradient at r = 0
-        const float4 xj = __ldg(a.xs + t);
+      const Cubic K(a.h);
+      const bool lists_ok = a.use_lists && lists_usable(a.L);
+      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                          [&](int t, float4 xj) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dist2_rn(dx, dy, dz);
-        if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+        float r, rinv;
+        r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
         const float4 vj = __ldg(a.vstar + t);
-        const float gs = K.dw_scale(sqrtf(r2));
-        d += vj.w * (gs * ((vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz));
+        const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+        d = fmaf(vj.w * K.grad_scale(r, rinv), vdot, d);
       });
     }
     a.d_rho_dt[i] = d;
@@ -277,7 +286,10 @@ __global__ void __launch_bounds__(kBlock) k_rate(RateArgs a) {
       kap = fminf((1.0f / a.dt) * dc * rf.x * rf.y, a.max_kappa);
       term = (double)dc;
     }
-    if (a.kappa_new) a.kappa_new[s] = kap;
+    if (a.kappa_new) {
+      a.kappa_new[s] = kap;
+      a.kratio_new[s] = kap / fmaxf(rf.x, 1.0e-6f);
+    }
     dyn = is_dyn ? 1 : 0;
   }
   if (!a.ctrl) return;
@@ -291,39 +303,38 @@ struct CorrectArgs {
   int64_t n;
   const float4* xs;
   float4* vstar;          // in/out (own slot only)
-  const float2* sc2;      // (rho, .)
-  const float* kappa;     // cell order
+  const float* kappa;     // cell order (committed to the API array)
+  const float* kratio;    // cell order kappa / max(rho, 1e-6)
   float h, dt;
   float* kappa_api;       // commit kappa to the API array (may be null)
   float* vstar_api;       // optional original-order v* output
+  NbrList L;
+  int use_lists;
   const DfsphDev* ctrl;
 };
 
-__global__ void __launch_bounds__(kBlock) k_correct(CorrectArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_correct(CorrectArgs a) {
   if (a.ctrl && a.ctrl->done) return;
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
   const int32_t i = a.g.perm[s];
-  const float ki = a.kappa[s];
-  if (a.kappa_api) a.kappa_api[i] = ki;
+  if (a.kappa_api) a.kappa_api[i] = a.kappa[s];
   float4 v = a.vstar[s];
   if (pf_of(xi) & PF_DYNAMIC) {
-    const CubicK K(a.h);
-    const float h2m = a.h * a.h * 1.000002f;
-    const float ci = ki / fmaxf(a.sc2[s].x, 1.0e-6f);
+    const Cubic K(a.h);
+    const float ci = a.kratio[s];
     float dvx = 0.f, dvy = 0.f, dvz = 0.f;
-    for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-      if (t == s) return;
-      const float4 xj = __ldg(a.xs + t);
+    const bool lists_ok = a.use_lists && lists_usable(a.L);
+    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t, float4 xj) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      const float r2 = dist2_rn(dx, dy, dz);
-      if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
-      const float coeff = __ldg(&a.vstar[t].w) * (ci + __ldg(a.kappa + t) / fmaxf(__ldg(&a.sc2[t].x), 1.0e-6f));
-      const float c = coeff * K.dw_scale(sqrtf(r2));
-      dvx += c * dx;
-      dvy += c * dy;
-      dvz += c * dz;
+      float r, rinv;
+      r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
+      const float c = __ldg(&a.vstar[t].w) * (ci + __ldg(a.kratio + t)) * K.grad_scale(r, rinv);
+      dvx = fmaf(c, dx, dvx);
+      dvy = fmaf(c, dy, dvy);
+      dvz = fmaf(c, dz, dvz);
     });
     v.x = v.x - a.dt * dvx;
     v.y = v.y - a.dt * dvy;
@@ -331,6 +342,13 @@ __global__ void __launch_bounds__(kBlock) k_correct(CorrectArgs a) {
     a.vstar[s] = v;
   }
   if (a.vstar_api) st3(a.vstar_api, i, xyz(v));
+}
+
+// kappa / max(rho, 1e-6) of gathered kappas (warm start, separate pass)
+__global__ void k_kappa_ratio(int64_t n, const float* __restrict__ kappa, const float2* __restrict__ sc2,
+                              float* __restrict__ kratio) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) kratio[s] = kappa[s] / fmaxf(sc2[s].x, 1.0e-6f);
 }
 
 // integrate_positions (341-353); also publishes v* in original order.
@@ -382,9 +400,12 @@ __global__ void k_residual(int64_t n, const int32_t* __restrict__ flags, const i
 }
 
 int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float dt, float max_kappa, float eta,
-             float* d_rho_dt, float* rho_star, float* kappa_new, DfsphDev* ctrl, cudaStream_t st) {
+             float* d_rho_dt, float* rho_star, float* kappa_new, float* kratio_new, DfsphDev* ctrl,
+             cudaStream_t st, bool use_lists = true) {
   RateArgs a;
   a.g = grid_view(c);
+  a.L = nbr_list(c);
+  a.use_lists = use_lists ? 1 : 0;
   a.n = m->n;
   a.xs = c->xs;
   a.vstar = c->vs2;
@@ -399,25 +420,30 @@ int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float 
   a.d_rho_dt = d_rho_dt;
   a.rho_star = rho_star;
   a.kappa_new = kappa_new;
+  a.kratio_new = kratio_new;
   a.ctrl = ctrl;
   a.red_part = c->red_part;
   a.red_cnt = c->red_cnt;
+  if (ctrl && blocks_for(a.n, kNbBlock) > reduction_blocks(c->capacity))
+    return set_error(FS_ERR_INVALID, "dfsph rate: reduction buffer too small");
   {
     PassScope ps_(c, P_DFSPH_RATE, st);
-    k_rate<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+    k_rate<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
   }
   return launch_check("dfsph rate");
 }
 
-int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float* kappa, float* kappa_api,
-                float* vstar_api, const DfsphDev* ctrl, cudaStream_t st) {
+int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float* kappa, const float* kratio,
+                float* kappa_api, float* vstar_api, const DfsphDev* ctrl, cudaStream_t st, bool use_lists = true) {
   CorrectArgs a;
   a.g = grid_view(c);
+  a.L = nbr_list(c);
+  a.use_lists = use_lists ? 1 : 0;
   a.n = m->n;
   a.xs = c->xs;
   a.vstar = c->vs2;
-  a.sc2 = c->sc2;
   a.kappa = kappa;
+  a.kratio = kratio;
   a.h = h;
   a.dt = dt;
   a.kappa_api = kappa_api;
@@ -425,7 +451,7 @@ int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float
   a.ctrl = ctrl;
   {
     PassScope ps_(c, P_DFSPH_CORRECT, st);
-    k_correct<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+    k_correct<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
   }
   return launch_check("dfsph correct");
 }
@@ -434,6 +460,7 @@ int run_density_factor(fs_context* c, const fs_model* m, float h, int min_nb, fl
                        int32_t* count, cudaStream_t st) {
   DensFactorArgs a;
   a.g = grid_view(c);
+  a.L = nbr_list(c);
   a.n = m->n;
   a.xs = c->xs;
   a.vs = c->vs2;
@@ -446,7 +473,7 @@ int run_density_factor(fs_context* c, const fs_model* m, float h, int min_nb, fl
   a.sc2 = c->sc2;
   {
     PassScope ps_(c, P_DFSPH_DENSITY_FACTOR, st);
-    k_density_factor<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+    k_density_factor<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
   }
   return launch_check("dfsph density/factor");
 }
@@ -494,6 +521,8 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
     return rc;
   AccelArgs aa;
   aa.g = grid_view(c);
+  aa.L = nbr_list(c);
+  aa.use_lists = 1;
   aa.n = n;
   aa.xs = c->xs;
   aa.vs = c->vs;
@@ -506,21 +535,22 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   aa.vstar = c->vs2;
   {
     PassScope ps_(c, P_DFSPH_ACCEL, st);
-    k_accel_predict<<<blocks_for(n), kBlock, 0, st>>>(aa);
+    k_accel_predict<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(aa);
   }
   if ((rc = launch_check("dfsph accel"))) return rc;
   if (p->warm_start) {
     {
-      PassScope ps_(c, P_GATHER, st);
+      PassScope ps_(c, P_GATHER, st, 2);
       k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa, c->sc1, nullptr);
+      k_kappa_ratio<<<blocks_for(n), kBlock, 0, st>>>(n, c->sc1, c->sc2, c->sc1b);
     }
-    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa, nullptr, nullptr, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa, nullptr, nullptr, st))) return rc;
   }
   for (int it = 0; it < p->max_rho_iterations; ++it) {
     if ((rc = run_rate(c, m, 0, it, h, dt, p->max_kappa, p->eta_density, so->d_rho_dt, so->rho_star, c->sc1,
-                       c->dfsph + 0, st)))
+                       c->sc1b, c->dfsph + 0, st)))
       return rc;
-    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa, nullptr, c->dfsph + 0, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa, nullptr, c->dfsph + 0, st))) return rc;
   }
   {
     PassScope ps_(c, P_DFSPH_INTEGRATE, st);
@@ -538,16 +568,17 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
     return rc;
   if (p->warm_start) {
     {
-      PassScope ps_(c, P_GATHER, st);
+      PassScope ps_(c, P_GATHER, st, 2);
       k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa_v, c->sc1, nullptr);
+      k_kappa_ratio<<<blocks_for(n), kBlock, 0, st>>>(n, c->sc1, c->sc2, c->sc1b);
     }
-    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa_v, nullptr, nullptr, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa_v, nullptr, nullptr, st))) return rc;
   }
   for (int it = 0; it < p->max_vel_iterations; ++it) {
     if ((rc = run_rate(c, m, 1, it, h, dt, p->max_kappa_v, p->eta_divergence, so->d_rho_dt, nullptr, c->sc1,
-                       c->dfsph + 1, st)))
+                       c->sc1b, c->dfsph + 1, st)))
       return rc;
-    if ((rc = run_correct(c, m, h, dt, c->sc1, so->kappa_v, nullptr, c->dfsph + 1, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa_v, nullptr, c->dfsph + 1, st))) return rc;
   }
   const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 1, 0.f, 0.f);
   {
@@ -596,7 +627,7 @@ int fs_dfsph_divergence(fs_context* c, const fs_model* m, const float* x, const 
   // rho/factor are not needed for the rate itself (mode 1 reads them only for kappa, which is discarded)
   if (cudaMemsetAsync(c->sc2, 0, sizeof(float2) * m->n, st) != cudaSuccess)
     return set_error(FS_ERR_CUDA, "fs_dfsph_divergence: memset");
-  return run_rate(c, m, 1, 0, h, 1.f, 0.f, 0.f, d_rho_dt, nullptr, nullptr, nullptr, st);
+  return run_rate(c, m, 1, 0, h, 1.f, 0.f, 0.f, d_rho_dt, nullptr, nullptr, nullptr, nullptr, st, false);
 }
 
 int fs_dfsph_correct(fs_context* c, const fs_model* m, const float* x, float* v_star, const float* rho,
@@ -610,7 +641,11 @@ int fs_dfsph_correct(fs_context* c, const fs_model* m, const float* x, float* v_
                                                        c->status);
   k_gather_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, rho, nullptr, c->sc2);
   k_gather_scalar<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, kappa, c->sc1, nullptr);
-  return run_correct(c, m, h, dt, c->sc1, nullptr, v_star, nullptr, st);
+  {
+    PassScope ps_(c, P_GATHER, st);
+    k_kappa_ratio<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->sc1, c->sc2, c->sc1b);
+  }
+  return run_correct(c, m, h, dt, c->sc1, c->sc1b, nullptr, v_star, nullptr, st, false);
 }
 
 int fs_dfsph_residual(fs_context* c, const fs_model* m, const float* a, const float* b, double* out,
@@ -620,6 +655,8 @@ int fs_dfsph_residual(fs_context* c, const fs_model* m, const float* a, const fl
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t n = m->n > 0 ? m->n : 1;
+  if (blocks_for(n) > reduction_blocks(c->capacity > 0 ? c->capacity : 1))
+    return set_error(FS_ERR_INVALID, "fs_dfsph_residual: reduction buffer too small");
   if (cudaMemsetAsync(c->dfsph, 0, sizeof(DfsphDev), st) != cudaSuccess)
     return set_error(FS_ERR_CUDA, "fs_dfsph_residual: memset");
   {

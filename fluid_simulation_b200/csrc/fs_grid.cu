@@ -16,7 +16,7 @@
 #include <cstdio>
 #include <cstring>
 
-#include "fs_internal.cuh"
+#include "fs_nbr.cuh"
 
 namespace fs {
 
@@ -37,6 +37,7 @@ __global__ void k_cell_keys(int64_t n, const float* __restrict__ x, float inv, i
   g.dim_x = dim_x;
   g.dim_y = dim_y;
   g.dim_z = dim_z;
+  g.mask_x = g.mask_y = g.mask_z = -1;
   const int k = phys_cell(g, to_cell(__fmul_rn(px, inv), rounding), to_cell(__fmul_rn(py, inv), rounding),
                           to_cell(__fmul_rn(pz, inv), rounding));
   key[i] = k;
@@ -143,7 +144,7 @@ __global__ void k_scatter(int64_t n, const int32_t* __restrict__ key, const int3
 }
 
 __global__ void k_rank(int64_t n, const int32_t* __restrict__ key, const int32_t* __restrict__ off,
-                       const int32_t* __restrict__ tmp, int32_t* __restrict__ perm) {
+                       const int32_t* __restrict__ tmp, int32_t* __restrict__ perm, int32_t* __restrict__ skey) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const int32_t i = tmp[s];
@@ -152,6 +153,7 @@ __global__ void k_rank(int64_t n, const int32_t* __restrict__ key, const int32_t
   int32_t rank = 0;
   for (int32_t t = a; t < b; ++t) rank += tmp[t] < i ? 1 : 0;
   perm[a + rank] = i;
+  skey[a + rank] = c;
 }
 
 __global__ void k_tables(int64_t n, int64_t ncell, const int32_t* __restrict__ perm, const int32_t* __restrict__ key,
@@ -161,7 +163,7 @@ __global__ void k_tables(int64_t n, int64_t ncell, const int32_t* __restrict__ p
   if (t < n) {
     const int32_t i = perm[t];
     if (point_ids) point_ids[t] = i;
-    if (point_cells) point_cells[t] = key[i];
+    if (point_cells) point_cells[t] = key[i];  // == skey[t]
   }
   if (t < ncell) {
     if (cell_starts) cell_starts[t] = off[t];
@@ -187,15 +189,30 @@ __global__ void k_candidates(GridDev g, const float* __restrict__ q, int64_t nq,
 
 int scan_blocks(int64_t m) { return (int)((m + kScanTile - 1) / kScanTile); }
 
+NbrList nbr_list(const fs_context* c) {
+  NbrList L;
+  L.idx = c->nb_idx;
+  L.cnt = c->nb_cnt;
+  L.stride = c->capacity > 0 ? c->capacity : 1;
+  L.ctl = (ListCtl*)c->nb_ctl;
+  return L;
+}
+
 GridDev grid_view(const fs_context* c) {
   GridDev g;
   g.off = c->cell_off;
   g.perm = c->perm;
+  g.skey = c->skey;
   g.dim_x = c->grid.dim_x;
   g.dim_y = c->grid.dim_y;
   g.dim_z = c->grid.dim_z;
   g.rounding = c->grid.rounding;
+  auto pow2mask = [](int d) { return (d & (d - 1)) == 0 ? d - 1 : -1; };
+  g.mask_x = pow2mask(g.dim_x);
+  g.mask_y = pow2mask(g.dim_y);
+  g.mask_z = pow2mask(g.dim_z);
   g.inv = c->built_inv;
+  g.tile_stats = c->tile_stats;
   return g;
 }
 
@@ -207,6 +224,9 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
   PassScope ps_(c, P_GRID, st, n > 0 ? 6 : 3);
   int rc = check_cuda(cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * c->ncell, st), "memset cell counts");
   if (rc) return rc;
+  // a new grid invalidates recorded neighbour lists
+  rc = check_cuda(cudaMemsetAsync(c->nb_ctl, 0, sizeof(ListCtl), st), "memset list control");
+  if (rc) return rc;
   if (n > 0)
     k_cell_keys<<<blocks_for(n), kBlock, 0, st>>>(n, x, inv, c->grid.dim_x, c->grid.dim_y, c->grid.dim_z,
                                                    c->grid.rounding, c->key, c->slot, c->cell_count, c->status);
@@ -216,7 +236,7 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
   k_scan_down<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, c->cell_off);
   if (n > 0) {
     k_scatter<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->slot, c->cell_off, c->tmp_ids);
-    k_rank<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->cell_off, c->tmp_ids, c->perm);
+    k_rank<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->cell_off, c->tmp_ids, c->perm, c->skey);
   }
   rc = launch_check("grid_build");
   if (rc) return rc;
@@ -279,6 +299,7 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
       {(void**)&c->key, sizeof(int32_t) * cap},         {(void**)&c->slot, sizeof(int32_t) * cap},
       {(void**)&c->cell_count, sizeof(int32_t) * ncell}, {(void**)&c->cell_off, sizeof(int32_t) * (ncell + 1)},
       {(void**)&c->tmp_ids, sizeof(int32_t) * cap},     {(void**)&c->perm, sizeof(int32_t) * cap},
+      {(void**)&c->skey, sizeof(int32_t) * cap},
       {(void**)&c->scan_part, sizeof(int32_t) * (nb + 1)},
       {(void**)&c->xs, sizeof(float4) * cap},           {(void**)&c->xs2, sizeof(float4) * cap},
       {(void**)&c->vs, sizeof(float4) * cap},           {(void**)&c->vs2, sizeof(float4) * cap},
@@ -287,6 +308,9 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
       {(void**)&c->xo_tmp, sizeof(float) * 3 * cap},    {(void**)&c->vo_tmp, sizeof(float) * 3 * cap},
       {(void**)&c->red_part, sizeof(double) * rb},      {(void**)&c->red_cnt, sizeof(int64_t) * rb},
       {(void**)&c->dfsph, sizeof(DfsphDev) * 2},         {(void**)&c->status, sizeof(uint32_t)},
+      {(void**)&c->tile_stats, sizeof(unsigned long long) * 8},
+      {(void**)&c->nb_idx, sizeof(int32_t) * kNbMax * cap},  {(void**)&c->nb_cnt, sizeof(int32_t) * cap},
+      {(void**)&c->nb_ctl, sizeof(ListCtl)},
   };
   for (auto& a : allocs) {
     cudaError_t e = cudaMalloc(a.p, a.bytes);
@@ -298,6 +322,8 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
   }
   int rc = check_cuda(cudaMemset(c->status, 0, sizeof(uint32_t)), "fs_context_create: memset");
   if (!rc) rc = check_cuda(cudaMemset(c->dfsph, 0, sizeof(DfsphDev) * 2), "fs_context_create: memset");
+  if (!rc) rc = check_cuda(cudaMemset(c->tile_stats, 0, sizeof(unsigned long long) * 8), "fs_context_create: memset");
+  if (!rc) rc = check_cuda(cudaMemset(c->nb_ctl, 0, sizeof(ListCtl)), "fs_context_create: memset");
   if (rc) {
     fs_context_destroy(c);
     return rc;
@@ -312,9 +338,9 @@ int fs_context_destroy(fs_context* c) {
   if (!c) return FS_OK;
   DeviceGuard dg(c->device);
   timer_free(c->timer);
-  void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->scan_part, c->xs, c->xs2,
+  void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
                 c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
-                c->dfsph, c->status};
+                c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete c;
@@ -443,6 +469,18 @@ int fs_status_read(fs_context* c, uint32_t* status) {
                       "fs_status_read");
   if (rc) return rc;
   return check_cuda(cudaStreamSynchronize(c->last_stream), "fs_status_read: sync");
+}
+
+int fs_list_stats(fs_context* c, int64_t* counters, int32_t ncounters, int32_t reset) {
+  if (!c || !counters || ncounters < 0) return set_error(FS_ERR_INVALID, "fs_list_stats: bad arguments");
+  DeviceGuard dg(c->device);
+  unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int rc = check_cuda(cudaStreamSynchronize(c->last_stream), "fs_list_stats: sync");
+  if (!rc) rc = check_cuda(cudaMemcpy(h, c->tile_stats, sizeof(h), cudaMemcpyDeviceToHost), "fs_list_stats");
+  if (rc) return rc;
+  for (int k = 0; k < ncounters && k < 8; ++k) counters[k] = (int64_t)h[k];
+  if (reset) rc = check_cuda(cudaMemset(c->tile_stats, 0, sizeof(h)), "fs_list_stats: reset");
+  return rc;
 }
 
 int fs_status_clear(fs_context* c, fs_stream_t stream) {

@@ -45,8 +45,11 @@ struct PassTimer {
 struct GridDev {
   const int32_t* off;   // [ncell + 1] exclusive prefix of cell occupancy (hash-key order)
   const int32_t* perm;  // [n] sorted slot -> original particle index (warp's point_ids)
+  const int32_t* skey;  // [n] cell key of each sorted slot (warp's point_cells)
   int32_t dim_x, dim_y, dim_z, rounding;
+  int32_t mask_x, mask_y, mask_z;  // dim - 1 when the dim is a power of two, else -1
   float inv;            // 1 / cell width, float32 as warp
+  unsigned long long* tile_stats;  // [2]: neighbour visits served by lists / by grid rescans
 };
 
 }  // namespace fs
@@ -67,6 +70,7 @@ struct fs_context {
   int32_t* cell_off = nullptr;   // [ncell + 1]
   int32_t* tmp_ids = nullptr;    // [cap] unordered-in-cell ids
   int32_t* perm = nullptr;       // [cap] sorted slot -> original index
+  int32_t* skey = nullptr;       // [cap] cell key of each sorted slot
   int32_t* scan_part = nullptr;  // [scan blocks + 1]
 
   // cell-sorted streams
@@ -86,6 +90,12 @@ struct fs_context {
   int64_t* red_cnt = nullptr;   // [reduction blocks]
   fs::DfsphDev* dfsph = nullptr; // [2] control blocks (density half, divergence half)
   uint32_t* status = nullptr;
+  unsigned long long* tile_stats = nullptr;  // [2] visits served by lists / by rescans
+
+  // neighbour lists (fs_nbr.cuh)
+  int32_t* nb_idx = nullptr;     // [kNbMax][cap]
+  int32_t* nb_cnt = nullptr;     // [cap]
+  void* nb_ctl = nullptr;        // ListCtl
 
   // instrumentation
   fs::PassTimer timer;
@@ -149,8 +159,11 @@ int reduction_blocks(int64_t n);
 
 constexpr float kPi = 3.14159265358979323846f;
 
-FS_DEV int pf_of(float4 p) { return __float_as_int(p.w); }
-FS_DEV float pack_pf(int pf) { return __int_as_float(pf); }
+// The .w word of a position: PF bits (a denormal, adds nothing measurable to
+// an r^2) for an active particle, +inf for an inactive one, so that an
+// r^2 + w test rejects inactive candidates without reading any flag.
+FS_DEV int pf_of(float4 p) { return __float_as_int(p.w) & (PF_ACTIVE | PF_DYNAMIC); }
+FS_DEV float pack_pf(int pf) { return __int_as_float((pf & PF_ACTIVE) ? pf : 0x7f800000); }
 
 // Distance computed with individually rounded operations (no FMA), so that
 // decisions such as `r < h` are bit-identical to a strict FP32 evaluation.
@@ -231,8 +244,16 @@ FS_DEV int wrap_axis(int v, int dim) {
   return v % dim;
 }
 
+// same, with a power-of-two mask when there is one (mask >= 0)
+FS_DEV int wrap_axis(int v, int dim, int mask) {
+  v += (1 << 20);
+  v = v < 0 ? 0 : v;
+  return mask >= 0 ? (v & mask) : v % dim;
+}
+
 FS_DEV int phys_cell(const GridDev& g, int x, int y, int z) {
-  return (wrap_axis(z, g.dim_z) * g.dim_y + wrap_axis(y, g.dim_y)) * g.dim_x + wrap_axis(x, g.dim_x);
+  return (wrap_axis(z, g.dim_z, g.mask_z) * g.dim_y + wrap_axis(y, g.dim_y, g.mask_y)) * g.dim_x +
+         wrap_axis(x, g.dim_x, g.mask_x);
 }
 
 // Visits the candidates of warp's hash_grid_query(grid, p, r) in the same
@@ -251,11 +272,11 @@ FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, f
   const int nx = x1 - x0 + 1;
   const int xa = x0 + (1 << 20);
   for (int z = z0; z <= z1; ++z) {
-    const int cz = wrap_axis(z, g.dim_z);
+    const int cz = wrap_axis(z, g.dim_z, g.mask_z);
     for (int y = y0; y <= y1; ++y) {
-      const int row = (cz * g.dim_y + wrap_axis(y, g.dim_y)) * g.dim_x;
+      const int row = (cz * g.dim_y + wrap_axis(y, g.dim_y, g.mask_y)) * g.dim_x;
       if (xa >= 0) {
-        const int cx0 = xa % g.dim_x;
+        const int cx0 = g.mask_x >= 0 ? (xa & g.mask_x) : xa % g.dim_x;
         const int len1 = min(nx, g.dim_x - cx0);
         int s = __ldg(g.off + row + cx0);
         int e = __ldg(g.off + row + cx0 + len1);
@@ -267,7 +288,7 @@ FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, f
         }
       } else {  // far outside the shifted range: cells clamp, visit one by one
         for (int x = x0; x <= x1; ++x) {
-          const int c = row + wrap_axis(x, g.dim_x);
+          const int c = row + wrap_axis(x, g.dim_x, g.mask_x);
           const int e = __ldg(g.off + c + 1);
           for (int t = __ldg(g.off + c); t < e; ++t) f(t);
         }

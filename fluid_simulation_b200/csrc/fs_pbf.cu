@@ -13,7 +13,7 @@
 //   xsph      XSPH viscosity, copy to state_out, apply_bounds      (fused)
 // As in the reference, the candidate set of every pass after the build is the
 // one binned at build time, queried from the particle's current position.
-#include "fs_internal.cuh"
+#include "fs_nbr.cuh"
 
 namespace fs {
 
@@ -48,34 +48,46 @@ __global__ void k_gather_xin(int64_t n, const int32_t* __restrict__ perm, const 
   out[s] = make_float4(p.x, p.y, p.z, 0.f);
 }
 
-// compute_density (115-141), poly6, self included.
-__global__ void __launch_bounds__(kBlock) k_density(GridDev g, int64_t n, const float4* __restrict__ xs,
-                                                    const float* __restrict__ mv, float h, float* rho,
-                                                    float2* __restrict__ sc2) {
+// compute_density (115-141), poly6, self included.  sc2[s] = (rho,
+// mass / max(rho, 1e-6)): the neighbour term of the viscosity and XSPH passes.
+// With `record` it records the neighbour lists that the next pass at the
+// same positions (accel, or XSPH) reuses.
+__global__ void __launch_bounds__(kNbBlock) k_density(GridDev g, NbrList L, int record, int64_t n,
+                                                      const float4* __restrict__ xs, const float4* __restrict__ vs,
+                                                      const float* __restrict__ mv, float h, float* rho,
+                                                      float2* __restrict__ sc2) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (record) lists_recorded(L);
   if (s >= n) return;
   const float4 xi = xs[s];
   const int32_t i = g.perm[s];
   float acc = 0.f;
+  const float h2m = h * h * kSupportMargin;
+  const Poly6Spiky K(h);
+  auto pair = [&](int t, float4 xj) {
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    acc = fmaf(__ldg(mv + t), K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz))), acc);
+  };
   if (pf_of(xi) & PF_ACTIVE) {
-    const PbfK K(h);
-    const float h2m = h * h * 1.000002f;
-    for_each_candidate(g, xi.x, xi.y, xi.z, h, [&](int t) {
-      const float4 xj = __ldg(xs + t);
-      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      const float r2 = dist2_rn(dx, dy, dz);
-      if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
-      acc += __ldg(mv + t) * K.w(sqrtf(r2));
-    });
+    if (record) {
+      record_list<false>(g, xs, (int)s, xi, h, h2m, L);
+      visit<true, true>(g, xs, (int)s, xi, h, h2m, L, true, pair);
+    } else {
+      scan_grid<true>(g, xs, (int)s, xi, h, h2m, pair);
+    }
+  } else if (record) {
+    L.cnt[s] = 0;
   }
   rho[i] = acc;
-  sc2[s] = make_float2(acc, 0.f);
+  sc2[s] = make_float2(acc, vs[s].w / fmaxf(acc, 1.0e-6f));
 }
 
 // acceleration_non_pressure (145-189, PBF branches) + apply_non_pressure_prediction
 // (228-242) + apply_position_bounds; writes the updated x_pred to xs_out.
 struct AccelArgs {
   GridDev g;
+  NbrList L;
+  int use_lists;
   int64_t n;
   const float4* xs;
   const float4* vs;
@@ -87,7 +99,7 @@ struct AccelArgs {
   float4* xs_out;
 };
 
-__global__ void __launch_bounds__(kBlock) k_accel_apply(AccelArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_accel_apply(AccelArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
@@ -101,31 +113,31 @@ __global__ void __launch_bounds__(kBlock) k_accel_apply(AccelArgs a) {
   const float mu = a.m.viscosity[i];
   const float gamma = a.m.surface_tension[i];
   const float coh = gamma / vi.w;
+  const float mu10 = 10.f * mu;
   const float visc_den_add = 0.01f * (a.h * a.h);
-  const PbfK K(a.h);
-  const float h2m = a.h * a.h * 1.000002f;
+  const float rp2 = a.particle_radius * a.particle_radius;
+  const Poly6Spiky K(a.h);
   float ax = 0.f, ay = 0.f, az = 0.f;
   if (gamma != 0.f || mu != 0.f) {
-    for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-      if (t == s) return;
-      const float4 xj = __ldg(a.xs + t);
+    const bool lists_ok = a.use_lists && lists_usable(a.L);
+    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t, float4 xj) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      const float r2 = dist2_rn(dx, dy, dz);
-      if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const float4 vj = __ldg(a.vs + t);
-      const float r = sqrtf(r2);
       float c = 0.f;
-      if (gamma != 0.f) c -= coh * vj.w * K.w(fmaxf(r, a.particle_radius));
+      if (gamma != 0.f) c -= coh * vj.w * K.w_r2(fmaxf(r2, rp2));  // W(max(r, r_p))
       if (mu != 0.f) {
-        const float vdot = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
+        const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
         if (vdot != 0.f) {
-          const float rho_j = __ldg(&a.sc2[t].x);
-          c += 10.f * mu * (vj.w / fmaxf(rho_j, 1.0e-6f)) * vdot / (r * r + visc_den_add) * K.dw_scale(r);
+          float r, rinv;
+          r_and_inv(r2, r, rinv);
+          c += mu10 * __ldg(&a.sc2[t].y) * __fdividef(vdot, r2 + visc_den_add) * K.grad_scale(r, rinv);
         }
       }
-      ax += c * dx;
-      ay += c * dy;
-      az += c * dz;
+      ax = fmaf(c, dx, ax);
+      ay = fmaf(c, dy, ay);
+      az = fmaf(c, dz, az);
     });
   }
   st3(a.accel, i, make_float3(ax, ay, az));
@@ -138,6 +150,8 @@ __global__ void __launch_bounds__(kBlock) k_accel_apply(AccelArgs a) {
 // compute_pbf_lambda (246-302)
 struct LambdaArgs {
   GridDev g;
+  NbrList L;
+  int use_lists;
   int64_t n;
   const float4* xs;
   const float4* vs;   // .w = mass
@@ -150,12 +164,14 @@ struct LambdaArgs {
   int32_t* count;     // API
 };
 
-__global__ void __launch_bounds__(kBlock) k_lambda(LambdaArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_lambda(LambdaArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  lists_recorded(a.L);
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
   const int32_t i = a.g.perm[s];
   if (!(pf_of(xi) & PF_DYNAMIC)) {
+    a.L.cnt[s] = 0;
     a.lam_s[s] = 0.f;
     if (a.lam) a.lam[i] = 0.f;
     if (a.rho) a.rho[i] = 0.f;
@@ -163,27 +179,29 @@ __global__ void __launch_bounds__(kBlock) k_lambda(LambdaArgs a) {
     return;
   }
   const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
-  const PbfK K(a.h);
-  const float h2m = a.h * a.h * 1.000002f;
+  const float inv_rho0 = 1.0f / rho0;
+  const Poly6Spiky K(a.h);
   float rho = 0.f, sq = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
   int cnt = 0;
-  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-    const float4 xj = __ldg(a.xs + t);
+  const float h2m = a.h * a.h * kSupportMargin;
+  // records the lists the delta pass of this iteration (same positions) reuses
+  record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
+  visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = dist2_rn(dx, dy, dz);
-    if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
-    const float r = sqrtf(r2);
-    if (t != s && r < a.h) ++cnt;
+    if (t != (int)s && exact_lt_h(dx, dy, dz, a.h, K.h2)) ++cnt;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float r, rinv;
+    r_and_inv(r2, r, rinv);
     const float mj = __ldg(&a.vs[t].w);
-    rho += mj * K.w(r);
-    const float c = -(mj / rho0) * K.dw_scale(r);
+    rho = fmaf(mj, K.w_r2(r2), rho);
+    const float c = -(mj * inv_rho0) * K.grad_scale(r, rinv);
     const float gjx = c * dx, gjy = c * dy, gjz = c * dz;
-    sq += gjx * gjx + gjy * gjy + gjz * gjz;
+    sq = fmaf(gjx, gjx, fmaf(gjy, gjy, fmaf(gjz, gjz, sq)));
     gx -= gjx;
     gy -= gjy;
     gz -= gjz;
   });
-  sq += gx * gx + gy * gy + gz * gz;
+  sq = fmaf(gx, gx, fmaf(gy, gy, fmaf(gz, gz, sq)));
   const float ci = fmaxf(rho / rho0 - 1.0f, 0.f);
   const float l = (a.min_nb > 0 && cnt < a.min_nb) ? 0.f : -ci / (sq + a.eps);
   a.lam_s[s] = l;
@@ -196,6 +214,8 @@ __global__ void __launch_bounds__(kBlock) k_lambda(LambdaArgs a) {
 // apply_delta_position (354-363) into xs_out (+ position bounds when asked).
 struct DeltaArgs {
   GridDev g;
+  NbrList L;
+  int use_lists;
   int64_t n;
   const float4* xs;
   const float4* vs;   // .w = mass
@@ -208,7 +228,7 @@ struct DeltaArgs {
   float4* xs_out;     // may be null (separate-pass use)
 };
 
-__global__ void __launch_bounds__(kBlock) k_delta(DeltaArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_delta(DeltaArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
@@ -220,23 +240,23 @@ __global__ void __launch_bounds__(kBlock) k_delta(DeltaArgs a) {
   }
   const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
   const float li = a.lam_s[s];
-  const PbfK K(a.h);
-  const float h2m = a.h * a.h * 1.000002f;
+  const Poly6Spiky K(a.h);
   const bool scorr = a.scorr_k != 0.f && !(a.w_dq <= 1.0e-6f);
+  const float inv_wdq = scorr ? 1.0f / a.w_dq : 0.f;
   float dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
-  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-    if (t == s) return;
-    const float4 xj = __ldg(a.xs + t);
+  const bool lists_ok = a.use_lists && lists_usable(a.L);
+  visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                      [&](int t, float4 xj) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = dist2_rn(dx, dy, dz);
-    if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
-    const float r = sqrtf(r2);
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float r, rinv;
+    r_and_inv(r2, r, rinv);
     float sc = 0.f;
-    if (scorr) sc = -a.scorr_k * powf(K.w(r) / a.w_dq, a.scorr_n);
-    const float c = (li + __ldg(a.lam_s + t) + sc) * __ldg(&a.vs[t].w) * K.dw_scale(r);
-    dx_ += c * dx;
-    dy_ += c * dy;
-    dz_ += c * dz;
+    if (scorr) sc = -a.scorr_k * powf(K.w_r2(r2) * inv_wdq, a.scorr_n);
+    const float c = (li + __ldg(a.lam_s + t) + sc) * __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
+    dx_ = fmaf(c, dx, dx_);
+    dy_ = fmaf(c, dy, dy_);
+    dz_ = fmaf(c, dz, dz_);
   });
   float3 d = make_float3(dx_ / rho0, dy_ / rho0, dz_ / rho0);
   if (a.max_dp > 0.f) {
@@ -273,6 +293,8 @@ __global__ void k_velocity(int64_t n, const float4* __restrict__ xs, const float
 // apply_xsph_viscosity (435-463) + copy x_pred -> particle_q + apply_bounds (467-517)
 struct XsphArgs {
   GridDev g;
+  NbrList L;
+  int use_lists;
   int64_t n;
   const float4* xs;
   const float4* vel;   // (v, mass) cell order
@@ -285,7 +307,7 @@ struct XsphArgs {
   float* x_pred_api;   // optional
 };
 
-__global__ void __launch_bounds__(kBlock) k_xsph_final(XsphArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_xsph_final(XsphArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
@@ -296,22 +318,20 @@ __global__ void __launch_bounds__(kBlock) k_xsph_final(XsphArgs a) {
   if (a.x_pred_api) st3(a.x_pred_api, i, p);
   if (pf_of(xi) & PF_DYNAMIC) {
     if (a.c > 0.f) {
-      const PbfK K(a.h);
-      const float h2m = a.h * a.h * 1.000002f;
+      const Poly6Spiky K(a.h);
       float cx = 0.f, cy = 0.f, cz = 0.f;
-      for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-        if (t == s) return;
-        const float4 xj = __ldg(a.xs + t);
+      const bool lists_ok = a.use_lists && lists_usable(a.L);
+      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                          [&](int t, float4 xj) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float r2 = dist2_rn(dx, dy, dz);
-        if (r2 > h2m || !(pf_of(xj) & PF_ACTIVE)) return;
         const float4 vj = __ldg(a.vel + t);
-        const float w = (vj.w / fmaxf(__ldg(&a.sc2[t].x), 1.0e-6f)) * K.w(sqrtf(r2));
-        cx += (vj.x - vi.x) * w;
-        cy += (vj.y - vi.y) * w;
-        cz += (vj.z - vi.z) * w;
+        // (m_j / max(rho_j, 1e-6)) W(r), the ratio from the final density pass
+        const float w = __ldg(&a.sc2[t].y) * K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        cx = fmaf(vj.x - vi.x, w, cx);
+        cy = fmaf(vj.y - vi.y, w, cy);
+        cz = fmaf(vj.z - vi.z, w, cz);
       });
-      v = make_float3(vi.x + a.c * cx, vi.y + a.c * cy, vi.z + a.c * cz);
+      v = make_float3(fmaf(a.c, cx, vi.x), fmaf(a.c, cy, vi.y), fmaf(a.c, cz, vi.z));
     }
     if (a.bounds) apply_walls(a.walls, p, v);
   }
@@ -332,9 +352,11 @@ __global__ void k_gather_lambda(int64_t n, const int32_t* __restrict__ perm, con
   if (s < n) out[s] = a[perm[s]];
 }
 
-__global__ void k_scalar_to_pair(int64_t n, const float* __restrict__ a, float2* __restrict__ out) {
+// (rho, mass / max(rho, 1e-6)) from a cell-order density and the mass in vel.w
+__global__ void k_rho_ratio(int64_t n, const float* __restrict__ rho, const float4* __restrict__ vel,
+                            float2* __restrict__ out) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n) out[s] = make_float2(a[s], 0.f);
+  if (s < n) out[s] = make_float2(rho[s], vel[s].w / fmaxf(rho[s], 1.0e-6f));
 }
 
 int gather_pbf(fs_context* c, const fs_model* m, const float* x_in, cudaStream_t st) {
@@ -384,12 +406,17 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   if ((rc = grid_build(c, c->xo_tmp, n, h, st))) return rc;
   if ((rc = gather_pbf(c, m, si->particle_q, st))) return rc;
   const GridDev g = grid_view(c);
+  // neighbour lists: density -> accel, lambda -> delta, final density -> XSPH
+  const NbrList L = nbr_list(c);
+  const int use_lists = 1;
   {
     PassScope ps_(c, P_PBF_DENSITY, st);
-    k_density<<<blocks_for(n), kBlock, 0, st>>>(g, n, c->xs, c->mv, h, so->rho, c->sc2);
+    k_density<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(g, L, 1, n, c->xs, c->vs, c->mv, h, so->rho, c->sc2);
   }
   AccelArgs aa;
   aa.g = g;
+  aa.L = L;
+  aa.use_lists = use_lists;
   aa.n = n;
   aa.xs = c->xs;
   aa.vs = c->vs;
@@ -403,7 +430,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   aa.xs_out = c->xs2;
   {
     PassScope ps_(c, P_PBF_ACCEL, st);
-    k_accel_apply<<<blocks_for(n), kBlock, 0, st>>>(aa);
+    k_accel_apply<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(aa);
   }
   if ((rc = launch_check("pbf accel"))) return rc;
   float4* cur = c->xs2;
@@ -412,6 +439,8 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     const GridDev gi = grid_view(c);
     LambdaArgs la;
     la.g = gi;
+    la.L = L;
+    la.use_lists = use_lists;
     la.n = n;
     la.xs = cur;
     la.vs = c->vs;
@@ -425,10 +454,12 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     la.count = so->neighbor_count;
     {
       PassScope ps_(c, P_PBF_LAMBDA, st);
-      k_lambda<<<blocks_for(n), kBlock, 0, st>>>(la);
+      k_lambda<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(la);
     }
     DeltaArgs da;
     da.g = gi;
+    da.L = L;
+    da.use_lists = use_lists;
     da.n = n;
     da.xs = cur;
     da.vs = c->vs;
@@ -445,7 +476,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     da.xs_out = nxt;
     {
       PassScope ps_(c, P_PBF_DELTA, st);
-      k_delta<<<blocks_for(n), kBlock, 0, st>>>(da);
+      k_delta<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(da);
     }
     if ((rc = launch_check("pbf iteration"))) return rc;
     float4* t = cur;
@@ -467,7 +498,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   const GridDev gf = grid_view(c);
   {
     PassScope ps_(c, P_PBF_DENSITY, st);
-    k_density<<<blocks_for(n), kBlock, 0, st>>>(gf, n, cur, c->mv, h, so->rho, c->sc2);
+    k_density<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(gf, L, 1, n, cur, c->vs, c->mv, h, so->rho, c->sc2);
   }
   {
     PassScope ps_(c, P_PBF_VELOCITY, st);
@@ -475,6 +506,8 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   }
   XsphArgs xa;
   xa.g = gf;
+  xa.L = L;
+  xa.use_lists = use_lists;
   xa.n = n;
   xa.xs = cur;
   xa.vel = nxt;
@@ -488,7 +521,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   xa.x_pred_api = x_pred;
   {
     PassScope ps_(c, P_PBF_XSPH, st);
-    k_xsph_final<<<blocks_for(n), kBlock, 0, st>>>(xa);
+    k_xsph_final<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(xa);
   }
   c->last_stream = st;
   return launch_check("pbf final");
@@ -500,9 +533,10 @@ int fs_pbf_density(fs_context* c, const fs_model* m, const float* x, float h, fl
   if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_pbf_density: build the grid first");
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
-  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, nullptr, c->xs, nullptr, c->mv,
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, x, c->xs, c->vs, c->mv,
                                                        c->status);
-  k_density<<<blocks_for(m->n), kBlock, 0, st>>>(grid_view(c), m->n, c->xs, c->mv, h, rho, c->sc2);
+  k_density<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(grid_view(c), nbr_list(c), 0, m->n, c->xs, c->vs, c->mv, h,
+                                                                rho, c->sc2);
   return launch_check("fs_pbf_density");
 }
 
@@ -517,6 +551,8 @@ int fs_pbf_lambda(fs_context* c, const fs_model* m, const float* x_pred, const f
                                                        c->status);
   LambdaArgs la;
   la.g = grid_view(c);
+  la.L = nbr_list(c);
+  la.use_lists = 0;
   la.n = m->n;
   la.xs = c->xs;
   la.vs = c->vs;
@@ -528,7 +564,7 @@ int fs_pbf_lambda(fs_context* c, const fs_model* m, const float* x_pred, const f
   la.lam = pbf_lambda;
   la.rho = rho;
   la.count = neighbor_count;
-  k_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(la);
+  k_lambda<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(la);
   return launch_check("fs_pbf_lambda");
 }
 
@@ -545,6 +581,8 @@ int fs_pbf_delta(fs_context* c, const fs_model* m, const float* x_pred, const fl
   k_gather_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, pbf_lambda, c->sc1);
   DeltaArgs da;
   da.g = grid_view(c);
+  da.L = nbr_list(c);
+  da.use_lists = 0;
   da.n = m->n;
   da.xs = c->xs;
   da.vs = c->vs;
@@ -559,7 +597,7 @@ int fs_pbf_delta(fs_context* c, const fs_model* m, const float* x_pred, const fl
   da.walls = Walls{};
   da.delta_p = delta_p;
   da.xs_out = nullptr;
-  k_delta<<<blocks_for(m->n), kBlock, 0, st>>>(da);
+  k_delta<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(da);
   return launch_check("fs_pbf_delta");
 }
 
@@ -573,9 +611,11 @@ int fs_pbf_xsph(fs_context* c, const fs_model* m, const float* x_pred, const flo
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, v_in, c->xs, c->vs2, nullptr,
                                                        c->status);
   k_gather_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, rho, c->sc1);
-  k_scalar_to_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->sc1, c->sc2);
+  k_rho_ratio<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->sc1, c->vs2, c->sc2);
   XsphArgs xa;
   xa.g = grid_view(c);
+  xa.L = nbr_list(c);
+  xa.use_lists = 0;
   xa.n = m->n;
   xa.xs = c->xs;
   xa.vel = c->vs2;
@@ -587,7 +627,7 @@ int fs_pbf_xsph(fs_context* c, const fs_model* m, const float* x_pred, const flo
   xa.x_out = nullptr;
   xa.v_out = v_out;
   xa.x_pred_api = nullptr;
-  k_xsph_final<<<blocks_for(m->n), kBlock, 0, st>>>(xa);
+  k_xsph_final<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(xa);
   return launch_check("fs_pbf_xsph");
 }
 

@@ -8,7 +8,7 @@
 //   force     pressure + viscosity + cohesion + gravity, then
 //             integrate_velocity, integrate_positions and apply_bounds fused
 //             -> accel, particle_qd, particle_q (original order)
-#include "fs_internal.cuh"
+#include "fs_nbr.cuh"
 
 namespace fs {
 
@@ -42,50 +42,52 @@ __global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_
 
 // ------------------------------------------------------------- density ----
 // compute_density_pressure, solver_wcsph.py:120-158.  Self included.
+// sc2[s] = (p / max(rho^2, 1e-6), 1 / max(rho, 1e-6)): the two per-particle
+// ratios of the force pass (cal_acc_with_pressure / _non_pressure).
 struct DensityArgs {
   GridDev g;
+  NbrList L;
   int64_t n;
   const float4* xs;
   const float* mv;
   const float* rest_density;  // original order
-  const float* stiffness;     // original order (nullptr: density only)
+  const float* stiffness;     // original order
   const float* exponent;
   float h;
   int clamp;
   float* rho;                 // original order (API)
-  float* pressure;            // original order (API), may be null
-  float2* sc2;                // cell order (rho, p)
+  float* pressure;            // original order (API)
+  float2* sc2;                // cell order
 };
 
-__global__ void __launch_bounds__(kBlock) k_wcsph_density(DensityArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_wcsph_density(DensityArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  lists_recorded(a.L);
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
   const int32_t i = a.g.perm[s];
   if (!(pf_of(xi) & PF_ACTIVE)) {
     a.rho[i] = 0.f;
-    if (a.pressure) a.pressure[i] = 0.f;
+    a.pressure[i] = 0.f;
     a.sc2[s] = make_float2(0.f, 0.f);
+    a.L.cnt[s] = 0;
     return;
   }
-  const CubicK K(a.h);
-  const float h2 = a.h * a.h;
+  const float h2m = a.h * a.h * kSupportMargin;
+  record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
+  const Cubic K(a.h);
   float acc = 0.f;
-  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-    const float4 xj = __ldg(a.xs + t);
+  visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = dist2_rn(dx, dy, dz);
-    if (r2 > h2 || !(pf_of(xj) & PF_ACTIVE)) return;  // W = 0 beyond the support
-    acc += __ldg(a.mv + t) * K.w(sqrtf(r2));
+    float r, rinv;
+    r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
+    acc = fmaf(__ldg(a.mv + t), K.w(r), acc);
   });
-  float p = 0.f;
-  if (a.stiffness) {
-    p = a.stiffness[i] * (powf(acc / fmaxf(a.rest_density[i], 1.0e-6f), a.exponent[i]) - 1.0f);
-    if (a.clamp) p = fmaxf(p, 0.f);
-    a.pressure[i] = p;
-  }
+  float p = a.stiffness[i] * (powf(acc / fmaxf(a.rest_density[i], 1.0e-6f), a.exponent[i]) - 1.0f);
+  if (a.clamp) p = fmaxf(p, 0.f);
   a.rho[i] = acc;
-  a.sc2[s] = make_float2(acc, p);
+  a.pressure[i] = p;
+  a.sc2[s] = make_float2(p / fmaxf(acc * acc, 1.0e-6f), 1.0f / fmaxf(acc, 1.0e-6f));
 }
 
 // --------------------------------------------------------------- force ----
@@ -93,6 +95,8 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_density(DensityArgs a) {
 // integrate_positions (248-260) + apply_bounds (264-305).
 struct ForceArgs {
   GridDev g;
+  NbrList L;
+  int use_lists;
   int64_t n;
   const float4* xs;
   const float4* vs;
@@ -105,7 +109,7 @@ struct ForceArgs {
   float* v_out;
 };
 
-__global__ void __launch_bounds__(kBlock) k_wcsph_force(ForceArgs a) {
+__global__ void __launch_bounds__(kNbBlock) k_wcsph_force(ForceArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
@@ -117,40 +121,34 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(ForceArgs a) {
     st3(a.x_out, i, xyz(xi));
     return;
   }
-  const float2 rp = a.sc2[s];
-  const float rho_i = rp.x, p_i = rp.y;
-  const float m_i = vi.w;
-  const float mu = a.m.viscosity[i];
-  const float gamma = a.m.surface_tension[i];
-  const float dp_i = p_i / fmaxf(rho_i * rho_i, 1.0e-6f);
-  const float coh = gamma / m_i;
+  const float dp_i = a.sc2[s].x;
+  const float mu10 = 10.f * a.m.viscosity[i];
+  const float coh = a.m.surface_tension[i] / vi.w;
   const float visc_den_add = 0.01f * (a.h * a.h);
-  const CubicK K(a.h);
-  const float h2 = a.h * a.h;
+  const Cubic K(a.h);
   float ax = 0.f, ay = 0.f, az = 0.f;
-  for_each_candidate(a.g, xi.x, xi.y, xi.z, a.h, [&](int t) {
-    if (t == s) return;
-    const float4 xj = __ldg(a.xs + t);
+  const bool lists_ok = a.use_lists && lists_usable(a.L);
+  visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                      [&](int t, float4 xj) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = dist2_rn(dx, dy, dz);
-    if (r2 > h2 || !(pf_of(xj) & PF_ACTIVE)) return;  // every term vanishes beyond h
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (r2 == 0.f) return;  // coincident particles: every term carries the zero vector d
     const float4 vj = __ldg(a.vs + t);
-    const float2 rpj = __ldg(a.sc2 + t);
-    const float r = sqrtf(r2);
+    const float2 rj = __ldg(a.sc2 + t);  // (p_j / rho_j^2, 1 / rho_j)
+    float r, rinv;
+    r_and_inv(r2, r, rinv);
     const float m_j = vj.w;
-    // cohesion: -gamma/m_i * m_j * d * W(max(r, r_p))
+    // cohesion -gamma/m_i m_j W(max(r, r_p)) d
     const float wc = coh * m_j * K.w(fmaxf(r, a.particle_radius));
-    // viscosity: 10 mu (m_j / max(rho_j,1e-6)) (v_ij . d) / (r^2 + 0.01 h^2) * gradW
-    const float vdot = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
-    const float gs = K.dw_scale(r);
-    const float visc = 10.f * mu * (m_j / fmaxf(rpj.x, 1.0e-6f)) * vdot / (r * r + visc_den_add);
-    // pressure: -m_j (p_i/rho_i^2 + p_j/rho_j^2) gradW
-    const float dp_j = rpj.y / fmaxf(rpj.x * rpj.x, 1.0e-6f);
-    const float pres = -m_j * (dp_i + dp_j);
-    const float c = (visc + pres) * gs - wc;
-    ax += c * dx;
-    ay += c * dy;
-    az += c * dz;
+    // viscosity 10 mu (m_j / rho_j) (v_ij . d) / (r^2 + 0.01 h^2) grad W
+    const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+    const float visc = mu10 * m_j * rj.y * __fdividef(vdot, r2 + visc_den_add);
+    // pressure -m_j (p_i / rho_i^2 + p_j / rho_j^2) grad W
+    const float pres = -m_j * (dp_i + rj.x);
+    const float c = fmaf(visc + pres, K.grad_scale(r, rinv), -wc);
+    ax = fmaf(c, dx, ax);
+    ay = fmaf(c, dy, ay);
+    az = fmaf(c, dz, az);
   });
   const float3 g = gravity_of(a.m, i);
   const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
@@ -171,6 +169,16 @@ __global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const
   out[s] = make_float2(a[i], b ? b[i] : 0.f);
 }
 
+// (rho, p) of original order -> force-pass ratios in cell order
+__global__ void k_gather_ratios(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ rho,
+                                const float* __restrict__ p, float2* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int32_t i = perm[s];
+  const float r = rho[i];
+  out[s] = make_float2(p[i] / fmaxf(r * r, 1.0e-6f), 1.0f / fmaxf(r, 1.0e-6f));
+}
+
 int wcsph_gather(fs_context* c, const fs_model* m, const float* x, const float* v, cudaStream_t st) {
   const int64_t n = m->n;
   {
@@ -184,11 +192,12 @@ int launch_density(fs_context* c, const fs_model* m, float h, int clamp, bool eo
                    cudaStream_t st) {
   DensityArgs a;
   a.g = grid_view(c);
+  a.L = nbr_list(c);
   a.n = m->n;
   a.xs = c->xs;
   a.mv = c->mv;
   a.rest_density = m->rest_density;
-  a.stiffness = eos ? m->stiffness : nullptr;
+  a.stiffness = m->stiffness;
   a.exponent = m->exponent;
   a.h = h;
   a.clamp = clamp;
@@ -197,15 +206,17 @@ int launch_density(fs_context* c, const fs_model* m, float h, int clamp, bool eo
   a.sc2 = c->sc2;
   {
     PassScope ps_(c, P_WCSPH_DENSITY, st);
-    k_wcsph_density<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+    k_wcsph_density<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
   }
   return launch_check("wcsph density");
 }
 
 int launch_force(fs_context* c, const fs_model* m, const fs_wcsph_params* p, float* accel, float* x_out,
-                 float* v_out, cudaStream_t st) {
+                 float* v_out, cudaStream_t st, bool use_lists) {
   ForceArgs a;
   a.g = grid_view(c);
+  a.L = nbr_list(c);
+  a.use_lists = use_lists ? 1 : 0;
   a.n = m->n;
   a.xs = c->xs;
   a.vs = c->vs;
@@ -220,7 +231,7 @@ int launch_force(fs_context* c, const fs_model* m, const fs_wcsph_params* p, flo
   a.v_out = v_out;
   {
     PassScope ps_(c, P_WCSPH_FORCE, st);
-    k_wcsph_force<<<blocks_for(a.n), kBlock, 0, st>>>(a);
+    k_wcsph_force<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
   }
   return launch_check("wcsph force");
 }
@@ -257,7 +268,7 @@ int fs_wcsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   if ((rc = grid_build(c, si->particle_q, m->n, h, st))) return rc;
   if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
   if ((rc = launch_density(c, m, h, p->clamp_negative_pressure, true, so->rho, so->pressure, st))) return rc;
-  return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st);
+  return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st, true);
 }
 
 int fs_wcsph_density(fs_context* c, const fs_model* m, const float* x, float h, int32_t clamp_negative, float* rho,
@@ -285,7 +296,7 @@ int fs_wcsph_force_integrate(fs_context* c, const fs_model* m, const fs_state* s
   if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
   k_gather_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, so->rho, so->pressure, c->sc2);
   if ((rc = launch_check("wcsph gather rho/p"))) return rc;
-  return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st);
+  return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st, false);
 }
 
 }  // extern "C"

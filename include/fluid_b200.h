@@ -221,6 +221,10 @@ const char* fs_pass_name(int32_t pass);
 int fs_timer_enable(fs_context* ctx, int32_t capacity); /* capacity 0 frees the events */
 int fs_timer_read(fs_context* ctx, float* ms_per_pass, int32_t* launches_per_pass, int32_t npass, int32_t* dropped);
 int64_t fs_launch_count(const fs_context* ctx);           /* kernels launched through ctx so far */
+/* Neighbour-list counters since the last reset (synchronises): [0] particle
+ * visits served by recorded lists, [1] visits that scanned the grid, [2] of
+ * those, scans because a recorded list overflowed. */
+int fs_list_stats(fs_context* ctx, int64_t* counters, int32_t ncounters, int32_t reset);
 
 /* ---- status ------------------------------------------------------------ */
 int fs_status_read(fs_context* ctx, uint32_t* status); /* synchronises the context's last stream */

@@ -41,31 +41,55 @@ def rel_err(a, b, scale=None):
     return float(np.abs(a - b).max()) / max(s, 1e-30)
 
 
-def field_scale(name, ref_sph, dt):
-    """Natural magnitude of a derived field, or None for max |field|.
+def compare_fields(pairs, ref64, tol=1e-5):
+    """Parity rule of the GPU tests.  pairs: (name, candidate, reference FP32);
+    ref64: name -> the FP64 oracle's value on the same inputs.
 
-    kappa_v = min((1/dt) max(drho/dt, 0) rho factor, cap): near convergence the
-    positive part of drho/dt is orders of magnitude below |drho/dt| itself, so
-    its FP32 error is measured against (1/dt) |rho factor drho/dt|."""
-    if name == "kappa_v" and {"rho", "factor", "d_rho_dt"} <= set(ref_sph):
-        r = np.asarray(ref_sph["rho"], np.float64) * np.asarray(ref_sph["factor"], np.float64)
-        return float(np.abs(r * np.asarray(ref_sph["d_rho_dt"], np.float64)).max()) / dt
-    return None
+    * integer fields (neighbor_count): identical;
+    * float fields: max|cand - ref| <= tol * max|ref|; or, for fields whose
+      own FP32 rounding exceeds that (quantities formed by cancellation:
+      EOS pressure near rest density, PBF lambda, DFSPH kappa_v, velocities
+      derived as position differences / dt, forces of nearly balanced
+      pressure), the candidate's distance from the FP64 solution is at most
+      4x the FP32 reference's own distance from it, or tol * max|FP64|.
+    Returns (errors, conditioned) lists of messages."""
+    errors, conditioned = [], []
+    for name, got, ref in pairs:
+        got = np.asarray(got)
+        ref = np.asarray(ref)
+        if name == "neighbor_count":
+            bad = int(np.count_nonzero(got != ref))
+            if bad:
+                errors.append(f"{name}: {bad} counts differ")
+            continue
+        e = rel_err(got, ref)
+        if e <= tol:
+            continue
+        r64 = ref64.get(name)
+        if r64 is None:
+            errors.append(f"{name}: rel err {e:.3e} (no FP64 reference)")
+            continue
+        r64 = np.asarray(r64, np.float64)
+        eg = float(np.abs(got.astype(np.float64) - r64).max())
+        er = float(np.abs(ref.astype(np.float64) - r64).max())
+        bound = max(tol * float(np.abs(r64).max()), 4.0 * er)
+        msg = f"{name}: rel err {e:.3e} vs FP32; |cand-FP64| {eg:.3e}, |FP32-FP64| {er:.3e}"
+        (conditioned if eg <= bound else errors).append(msg)
+    return errors, conditioned
 
 
-def velocity_scale(v_ref, x_ref, dt, tol):
-    """PBF sets v = (x_pred - x_in) / dt: a difference of O(|x|) positions, so a
-    few-ulp position difference becomes eps32 |x| / dt in v.  The scale keeps
-    the tolerance at tol relative to |v| but never below 4 ulp(|x|) / dt."""
-    vmax = float(np.abs(v_ref).max())
-    xmax = float(np.abs(x_ref).max())
-    return max(vmax, 4.0 * float(np.finfo(np.float32).eps) * xmax / (dt * tol))
-
-
-# PBF lambda = -max(rho/rho0 - 1, 0) / (sum |grad C|^2 + eps) subtracts two O(1)
-# numbers: a density agreeing to FP32 rounding (relative 1e-7..1e-6) moves C
-# by that much, i.e. by (rho/rho0) / C relative in lambda, ~1e2 at the dam's
-# 1 % compression.  Lambda and the Jacobi correction delta_p built from it
-# are therefore held to 1e-3 of their maximum, while the particle positions,
-# velocities and densities they produce stay within 1e-5.
-CONDITIONED_TOL = {"pbf_lambda": 1e-3, "delta_p": 1e-3}
+def oracle_outputs(kind, model, state_in, cfg, dt, precision):
+    """Flat name -> array dict of one oracle step."""
+    import oracle
+    if kind == "wcsph":
+        out, acc = oracle.wcsph_step(model, state_in, cfg, dt, precision=precision)
+        extra = {}
+    elif kind == "dfsph":
+        out, acc, _ = oracle.dfsph_step(model, state_in, cfg, dt, precision=precision)
+        extra = {}
+    else:
+        out, acc, xp = oracle.pbf_step(model, state_in, cfg, dt, precision=precision)
+        extra = {"x_pred": xp}
+    flat = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], accel=acc, **extra)
+    flat.update(out["sph"])
+    return flat
