@@ -107,6 +107,8 @@ SIGNATURES = {
     "fs_timer_read": (C.c_int, [P, P, P, I32, P]),
     "fs_launch_count": (I64, [P]),
     "fs_list_stats": (C.c_int, [P, P, I32, I32]),
+    "fs_noalloc_max_particles": (I32, []),
+    "fs_wcsph_density_noalloc": (C.c_int, [C.POINTER(Model), P, F, I32, P, P, P]),
     "fs_status_read": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "fs_status_clear": (C.c_int, [P, P]),
     "fs_last_error_string": (C.c_char_p, []),

@@ -226,6 +226,22 @@ int64_t fs_launch_count(const fs_context* ctx);           /* kernels launched th
  * those, scans because a recorded list overflowed. */
 int fs_list_stats(fs_context* ctx, int64_t* counters, int32_t ncounters, int32_t reset);
 
+/* ---- allocation-free density (no counterpart in the reference) ----------
+ * For callers that cannot allocate device memory (hosts whose allocator
+ * forbids cudaMalloc, plugins inside a runtime that owns all device memory,
+ * work recorded into a CUDA graph): grid build + WCSPH density and EOS, the
+ * results of fs_grid_build + fs_wcsph_density (up to summation order), in a
+ * fixed scratch area compiled into the library (about 1 MB per GPU that loads
+ * it, held until exit) instead of an fs_context.  At most
+ * fs_noalloc_max_particles() particles; larger n returns FS_ERR_CAPACITY.
+ * The first call on each device looks up the scratch address
+ * (cudaGetSymbolAddress); make that call before any stream capture.  All
+ * calls share the one scratch area: calls whose work overlaps on the GPU
+ * (other streams, other host threads) race and give wrong results. */
+int32_t fs_noalloc_max_particles(void);
+int fs_wcsph_density_noalloc(const fs_model* model, const float* x, float h, int32_t clamp_negative, float* rho,
+                             float* pressure, fs_stream_t stream);
+
 /* ---- status ------------------------------------------------------------ */
 int fs_status_read(fs_context* ctx, uint32_t* status); /* synchronises the context's last stream */
 int fs_status_clear(fs_context* ctx, fs_stream_t stream);
