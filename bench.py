@@ -53,6 +53,10 @@ B_ALG = {
     "dfsph_accel": 76, "dfsph_rate": 60, "dfsph_correct": 56, "dfsph_integrate": 36, "dfsph_final": 48,
 }
 PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 4090 (performance_summary.json)
+# DRAM bytes (read + write) per particle per launch from one full ncu capture
+# (cold cache), profiles/pbf_dam_401856.md: k_lambda 26.0 MB + 12.4 MB at
+# 401,856 particles.
+TRAFFIC_PER_PARTICLE = {"pbf_lambda": 38.3e6 / 401856}
 FALLBACK_HBM_GBS = 6650.0
 SUBSTEP_DT = {"pbf": 1.0 / 240.0, "dfsph": 1.0 / 240.0}
 
@@ -88,20 +92,24 @@ def build_workload(name, device):
         else:
             desc.update(max_rho_iterations=5, max_vel_iterations=12, warm_start=False)
         return m, solver, SUBSTEP_DT[kind], s.count, desc
-    if name == "wcsph_stress_4m":
-        x, v, sp = stress_lattice(cells=128, box=1.6)   # BCC: 2 * 128^3 = 4,194,304 at d = 9.92 mm
+    if name in ("wcsph_stress_4m", "wcsph_stress_524k"):
+        # BCC: 2 * 128^3 = 4,194,304 at d = 9.92 mm; the 524k variant (2 * 64^3 in a 0.8 m cube,
+        # same spacing) is the small case of the profiling captures
+        cells, box = (128, 1.6) if name == "wcsph_stress_4m" else (64, 0.8)
+        x, v, sp = stress_lattice(cells=cells, box=box)
         m = model_from_arrays(x, v, 1000.0 * sp ** 3, device=device, radius=0.5 * sp,
                               attributes=dict(rest_density=1000.0, surface_tension=0.0, viscosity=1e-6,
                                               stiffness=2.5e5, exponent=7.0, particle_mask=0), solver_cls=SolverWCSPH)
+        half = 0.5 * box
         solver = SolverWCSPH(m, SolverWCSPH.SphConfig(particle_radius=0.5 * sp, particle_length=sp,
                                                       smoothing_length_coff=2.0, boundary_damping=0.0,
-                                                      bound_width=0.8, bound_height=0.8, bound_length=0.8))
+                                                      bound_width=half, bound_height=half, bound_length=half))
         c0 = (2.5e5 * 7.0 / 1000.0) ** 0.5
         h = 2.0 * sp
         dt = 0.25 * h / (c0 + float(np.linalg.norm(v, axis=1).max()))
-        return m, solver, dt, len(x), dict(workload=name, particles=len(x), scene="jittered BCC lattice 2 x 128^3 "
-                                           "filling [-0.8,0.8]^2 x [0,1.6] m, v ~ N(0, 0.2)", solver="WCSPH", dt=dt,
-                                           h=h, spacing=sp)
+        return m, solver, dt, len(x), dict(workload=name, particles=len(x), scene=f"jittered BCC lattice 2 x {cells}^3 "
+                                           f"filling [-{half},{half}]^2 x [0,{box}] m, v ~ N(0, 0.2)", solver="WCSPH",
+                                           dt=dt, h=h, spacing=sp)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -269,7 +277,8 @@ def run_ours(args):
     achieved = bpl / (passes[dom]["ms_avg"] * 1e-3) / 1e9
     roofline = dict(bound="hbm", kernel=dom, achieved=round(achieved, 1), peak=peak, unit="GB/s",
                     frac=round(achieved / peak, 4), peak_source=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                    traffic=None, bytes_per_launch=bpl,
+                    traffic=(round(TRAFFIC_PER_PARTICLE[dom] * n) if dom in TRAFFIC_PER_PARTICLE else None),
+                    bytes_per_launch=bpl,
                     share_of_step=round(passes[dom]["ms_total"] / max(step_ms, 1e-9), 3))
     all_passes_b = sum(B_ALG.get(k, 0) * n * v["launches"] for k, v in passes.items())
     step_roofline = dict(algorithmic_bytes_per_step=all_passes_b / K, achieved_gbs=round(
@@ -329,7 +338,7 @@ def run_ours(args):
             torch.cuda.empty_cache()
 
     cpu = None
-    if world == 1 and not args.no_cpu_baseline and args.workload != "wcsph_stress_4m":
+    if world == 1 and not args.no_cpu_baseline and not args.workload.startswith("wcsph_stress"):
         cpu = time_cpu_baseline(args.workload, max_seconds=args.cpu_seconds)
 
     if rank == 0:
@@ -357,7 +366,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    if args.workload == "wcsph_stress_4m":
+    if args.workload.startswith("wcsph_stress"):
         raise SystemExit("the reference arm covers the dam-break workloads")
     kind, model, state, cfg, n = cpu_oracle_setup(args.workload)
     import oracle
@@ -395,7 +404,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pbf_dam_401856",
-                    choices=["pbf_dam_401856", "dfsph_dam_401856", "wcsph_stress_4m"])
+                    choices=["pbf_dam_401856", "dfsph_dam_401856", "wcsph_stress_4m", "wcsph_stress_524k"])
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
