@@ -37,6 +37,11 @@ class GridConfig(C.Structure):
     _fields_ = [("dim_x", I32), ("dim_y", I32), ("dim_z", I32), ("rounding", I32)]
 
 
+class WorldBox(C.Structure):
+    _fields_ = [("cell_lo", I32 * 3), ("dims", I32 * 3), ("bound_width", F), ("bound_height", F),
+                ("bound_length", F)]
+
+
 class Model(C.Structure):
     _fields_ = [("n", I64), ("n_worlds", I32)] + [(k, P) for k in (
         "particle_flags", "particle_mask", "particle_world", "particle_mass", "gravity", "rest_density",
@@ -81,6 +86,11 @@ SIGNATURES = {
     "fs_grid_build": (C.c_int, [P, P, I64, F, P]),
     "fs_grid_tables": (C.c_int, [P, P, P, P, P, P]),
     "fs_grid_candidates": (C.c_int, [P, P, I64, F, P, P, P, P]),
+    "fs_context_create_worlds": (C.c_int, [C.POINTER(P), I64, C.POINTER(WorldBox), I32, I32]),
+    "fs_context_worlds": (I32, [P]),
+    "fs_context_cells": (I64, [P]),
+    "fs_grid_build_worlds": (C.c_int, [P, P, P, I64, F, P]),
+    "fs_grid_candidates_worlds": (C.c_int, [P, P, P, I64, F, P, P, P, P]),
     "fs_wcsph_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
                                    C.POINTER(WcsphParams), P, P]),
     "fs_dfsph_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),

@@ -1,0 +1,183 @@
+"""Batches of independent dam-break scenes that advance in one model.
+
+Each scene is one Newton world (``Model.particle_world``): its own tank
+[-W, W] x [-H, H] x [0, 2L] with the reference dam-break proportions
+(W : H : L = 1.2 : 0.28 : 0.6, examples/dam_break/simulation.py:86-92) scaled
+to the scene, its own water column (a fraction of the tank along x, full
+width, height L, as the reference column x in [-1.2, -0.6], z in [0, 0.6]),
+and its own stiffness and viscosity.  All scenes share the particle spacing,
+hence h, mass and dt, so one solver config steps them all.  Scenes overlap in
+space (every tank starts at the origin); the segmented grid
+(``newton_shim.WorldGrid``) keeps them apart.
+
+``make_batch`` draws the scene set from one seed:
+  N_s = exp(U(ln n_lo, ln n_hi))  particles of scene s (before lattice rounding)
+  f_s ~ U(0.2, 0.6)              column length / tank length along x
+  k_s, m_s ~ U(0.8, 1.2)         stiffness and viscosity factors
+then fills each column with a cell-centred cubic lattice at ``spacing``,
+jittered by U(-1 %, 1 %) of the spacing from default_rng((seed, s)).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# reference dam-break tank proportions and material (simulation.py:86-132)
+TANK = (1.2, 0.28, 0.6)
+REST_DENSITY = 1000.0
+STIFFNESS = 2.5e5
+VISCOSITY = 1.0e-6
+EXPONENT = 7.0
+GRAVITY = (0.0, 0.0, -10.0)
+
+
+@dataclass
+class Scene:
+    count: int
+    walls: tuple          # (bound_width, bound_height, bound_length)
+    column_fraction: float
+    stiffness: float
+    viscosity: float
+    x: np.ndarray         # [count, 3] float32
+
+
+@dataclass
+class Batch:
+    spacing: float
+    scenes: list = field(default_factory=list)
+
+    # shared material / solver scalars ------------------------------------
+    @property
+    def h(self) -> float:
+        return 2.0 * self.spacing
+
+    @property
+    def mass(self) -> float:
+        return REST_DENSITY * self.spacing ** 3
+
+    @property
+    def radius(self) -> float:
+        return 0.5 * self.spacing
+
+    # concatenated arrays -------------------------------------------------
+    @property
+    def counts(self) -> np.ndarray:
+        return np.array([s.count for s in self.scenes], np.int64)
+
+    @property
+    def starts(self) -> np.ndarray:
+        return np.concatenate([[0], np.cumsum(self.counts)])
+
+    @property
+    def total(self) -> int:
+        return int(self.counts.sum())
+
+    def positions(self) -> np.ndarray:
+        return np.concatenate([s.x for s in self.scenes]).astype(np.float32)
+
+    def world(self) -> np.ndarray:
+        return np.repeat(np.arange(len(self.scenes), dtype=np.int32), self.counts)
+
+    def per_particle(self, name: str) -> np.ndarray:
+        return np.repeat(np.array([getattr(s, name) for s in self.scenes], np.float32), self.counts)
+
+    def boxes(self, h: float | None = None):
+        """WorldGrid boxes: the cells int(x / h) (truncating, float32 as the
+        device computes them) that the tank of each scene spans."""
+        h = self.h if h is None else h
+        inv = np.float32(1.0) / np.float32(h)
+        out = []
+        for s in self.scenes:
+            w, hh, l = s.walls
+            lo = [int(np.float32(v) * inv) for v in (-w, -hh, 0.0)]
+            hi = [int(np.float32(v) * inv) for v in (w, hh, 2.0 * l)]
+            out.append((tuple(lo), tuple(b - a + 1 for a, b in zip(lo, hi)), s.walls))
+        return out
+
+    def attributes(self, wcsph: bool = True) -> dict:
+        n = self.total
+        a = dict(particle_mask=0, rest_density=np.full(n, REST_DENSITY, np.float32),
+                 surface_tension=np.zeros(n, np.float32), viscosity=self.per_particle("viscosity"))
+        if wcsph:
+            a.update(stiffness=self.per_particle("stiffness"), exponent=np.full(n, EXPONENT, np.float32))
+        return a
+
+
+def scene_column(count_target: int, fraction: float, spacing: float, rng) -> tuple:
+    """Tank walls and jittered lattice of one scene."""
+    a = (count_target * spacing ** 3 / (4.0 * TANK[0] * TANK[1] * TANK[2] * fraction)) ** (1.0 / 3.0)
+    w, hh, l = (TANK[0] * a, TANK[1] * a, TANK[2] * a)
+    lo = np.array([-w, -hh, 0.0])
+    ext = np.array([2.0 * w * fraction, 2.0 * hh, l])
+    res = [max(1, int(round(e / spacing))) for e in ext]
+    axes = [lo[k] + (np.arange(res[k]) + 0.5) * spacing for k in range(3)]
+    g = np.meshgrid(*axes, indexing="ij")
+    x = np.stack([t.ravel() for t in g], 1)
+    x += rng.uniform(-0.01, 0.01, x.shape) * spacing
+    # the lattice may overhang the rounded column by < spacing / 2: keep it in the tank
+    x[:, 0] = np.clip(x[:, 0], -w, w)
+    x[:, 1] = np.clip(x[:, 1], -hh, hh)
+    return (float(w), float(hh), float(l)), x.astype(np.float32)
+
+
+def make_batch(n_scenes: int = 256, seed: int = 3, n_lo: int = 2000, n_hi: int = 100000,
+               spacing: float = 0.01) -> Batch:
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), n_scenes))
+    frac = rng.uniform(0.2, 0.6, n_scenes)
+    kf = rng.uniform(0.8, 1.2, n_scenes)
+    mf = rng.uniform(0.8, 1.2, n_scenes)
+    b = Batch(spacing=float(spacing))
+    for s in range(n_scenes):
+        walls, x = scene_column(float(counts[s]), float(frac[s]), spacing, np.random.default_rng((seed, s)))
+        b.scenes.append(Scene(len(x), walls, float(frac[s]), float(STIFFNESS * kf[s]), float(VISCOSITY * mf[s]), x))
+    return b
+
+
+def batched_model(batch: Batch, solver_cls, device="cuda:0", v=None):
+    """Model + WorldGrid of the whole batch (one world per scene)."""
+    from .newton_shim import WorldGrid, model_from_arrays
+
+    x = batch.positions()
+    m = model_from_arrays(x, np.zeros_like(x) if v is None else v, batch.mass, device=device,
+                          world=batch.world(), gravity=[GRAVITY] * len(batch.scenes), radius=batch.radius,
+                          attributes=batch.attributes(wcsph=solver_cls.__name__ == "SolverWCSPH"),
+                          solver_cls=solver_cls)
+    m.particle_grid = WorldGrid(batch.boxes(), device=device)
+    m.particle_grid.reserve(m.particle_count)
+    return m
+
+
+def scene_model(batch: Batch, k: int, solver_cls, device="cuda:0", v=None):
+    """Model of scene k alone (plain hash grid), for serial runs and parity."""
+    from .newton_shim import model_from_arrays
+
+    s = batch.scenes[k]
+    n = s.count
+    attrs = dict(particle_mask=0, rest_density=REST_DENSITY, surface_tension=0.0, viscosity=s.viscosity)
+    if solver_cls.__name__ == "SolverWCSPH":
+        attrs.update(stiffness=s.stiffness, exponent=EXPONENT)
+    return model_from_arrays(s.x, np.zeros_like(s.x) if v is None else v, batch.mass, device=device,
+                             world=np.zeros(n, np.int32), gravity=[GRAVITY], radius=batch.radius, attributes=attrs,
+                             solver_cls=solver_cls)
+
+
+def shard_scenes(counts, world_size: int) -> list:
+    """Scenes per rank for a batched run on several GPUs: scenes are
+    independent, so ranks share no particles and exchange nothing.  Greedy
+    longest-first assignment to the least-loaded rank balances the particle
+    counts (within the largest scene of the mean)."""
+    counts = np.asarray(counts, np.int64)
+    load = np.zeros(world_size, np.int64)
+    out = [[] for _ in range(world_size)]
+    for s in np.argsort(-counts, kind="stable"):
+        r = int(np.argmin(load))
+        out[r].append(int(s))
+        load[r] += counts[s]
+    return [sorted(o) for o in out]
+
+
+def sub_batch(batch: Batch, scenes) -> Batch:
+    return Batch(spacing=batch.spacing, scenes=[batch.scenes[k] for k in scenes])

@@ -19,14 +19,21 @@ namespace fs {
 // any block size used here).
 int reduction_blocks(int64_t n) { return blocks_for(n > 0 ? n : 1, 64); }
 
-// gathers of fs_wcsph.cu reused here
+// gather of fs_wcsph.cu reused here
 __global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
                                 const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
-                                float* __restrict__ mv, uint32_t* status);
-__global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
-                              const float* __restrict__ b, float2* __restrict__ out);
+                                float* __restrict__ mv, uint32_t* status, int nworlds);
 
 namespace {
+
+// (a[i], b[i]) of original order into cell order
+__global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
+                              const float* __restrict__ b, float2* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int32_t i = perm[s];
+  out[s] = make_float2(a[i], b ? b[i] : 0.f);
+}
 
 __global__ void k_gather_scalar(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
                                 float* __restrict__ out, float* __restrict__ copy_to) {
@@ -498,6 +505,9 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   if (p->warm_start && (!si->kappa || !si->kappa_v))
     return set_error(FS_ERR_INVALID, "fs_dfsph_substep: warm_start needs state_in kappa/kappa_v");
   if (m->n > c->capacity) return set_error(FS_ERR_CAPACITY, "fs_dfsph_substep: n > capacity");
+  if (c->worlds)
+    return set_error(FS_ERR_INVALID, "fs_dfsph_substep: the DFSPH iteration decisions are global; batched "
+                                     "contexts run WCSPH and PBF");
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t n = m->n;
@@ -505,11 +515,11 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   int rc;
   if ((rc = check_cuda(cudaMemsetAsync(c->dfsph, 0, sizeof(DfsphDev) * 2, st), "dfsph reset"))) return rc;
   // ---- first half: positions x_in
-  if ((rc = grid_build(c, si->particle_q, n, h, st))) return rc;
+  if ((rc = grid_build(c, si->particle_q, n, h, st, nullptr))) return rc;
   {
     PassScope ps_(c, P_GATHER, st);
     k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, si->particle_q, si->particle_qd, c->xs, c->vs,
-                                                    c->mv, c->status);
+                                                    c->mv, c->status, c->nworlds);
   }
   {
     // density/factor reads masses from vs2.w: fill it from vs (v_in, mass) first
@@ -558,11 +568,11 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   }
   if ((rc = launch_check("dfsph integrate"))) return rc;
   // ---- second half: positions x_out
-  if ((rc = grid_build(c, so->particle_q, n, h, st))) return rc;
+  if ((rc = grid_build(c, so->particle_q, n, h, st, nullptr))) return rc;
   {
     PassScope ps_(c, P_GATHER, st);
     k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, so->particle_q, so->v_star, c->xs, c->vs2, c->mv,
-                                                    c->status);
+                                                    c->status, c->nworlds);
   }
   if ((rc = run_density_factor(c, m, h, p->min_neighbors_for_factor, so->rho, so->factor, so->neighbor_count, st)))
     return rc;
@@ -612,7 +622,7 @@ int fs_dfsph_density_factor(fs_context* c, const fs_model* m, const float* x, fl
   if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_dfsph_density_factor: build the grid first");
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
-  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, x, c->xs, c->vs2, c->mv, c->status);
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, x, c->xs, c->vs2, c->mv, c->status, c->nworlds);
   return run_density_factor(c, m, h, min_nb, rho, factor, neighbor_count, st);
 }
 
@@ -623,7 +633,7 @@ int fs_dfsph_divergence(fs_context* c, const fs_model* m, const float* x, const 
   if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_dfsph_divergence: build the grid first");
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
-  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, v, c->xs, c->vs2, nullptr, c->status);
+  k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, v, c->xs, c->vs2, nullptr, c->status, c->nworlds);
   // rho/factor are not needed for the rate itself (mode 1 reads them only for kappa, which is discarded)
   if (cudaMemsetAsync(c->sc2, 0, sizeof(float2) * m->n, st) != cudaSuccess)
     return set_error(FS_ERR_CUDA, "fs_dfsph_divergence: memset");
@@ -638,7 +648,7 @@ int fs_dfsph_correct(fs_context* c, const fs_model* m, const float* x, float* v_
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, v_star, c->xs, c->vs2, nullptr,
-                                                       c->status);
+                                                       c->status, c->nworlds);
   k_gather_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, rho, nullptr, c->sc2);
   k_gather_scalar<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, kappa, c->sc1, nullptr);
   {

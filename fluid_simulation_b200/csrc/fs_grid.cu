@@ -44,6 +44,22 @@ __global__ void k_cell_keys(int64_t n, const float* __restrict__ x, float inv, i
   slot[i] = atomicAdd(count + k, 1);
 }
 
+// Batched contexts: key = (world, cell) as the world's base + its local cell.
+__global__ void k_cell_keys_worlds(int64_t n, const float* __restrict__ x, const int32_t* __restrict__ world,
+                                   const WorldDev* __restrict__ worlds, int nworlds, float inv,
+                                   int32_t* __restrict__ key, int32_t* __restrict__ slot,
+                                   int32_t* __restrict__ count, uint32_t* status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
+  if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(status, FS_STATUS_NONFINITE);
+  const int w = world[i];
+  if (w < 0 || w >= nworlds) atomicOr(status, FS_STATUS_BOUNDS);
+  const int k = world_cell_key(worlds[world_index(w, nworlds)], inv, px, py, pz);
+  key[i] = k;
+  slot[i] = atomicAdd(count + k, 1);
+}
+
 // phase 1: per-tile sums
 __global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t m, int32_t* __restrict__ part) {
   __shared__ int32_t warp_sums[kScanThreads / 32];
@@ -172,13 +188,14 @@ __global__ void k_tables(int64_t n, int64_t ncell, const int32_t* __restrict__ p
 }
 
 template <bool FILL>
-__global__ void k_candidates(GridDev g, const float* __restrict__ q, int64_t nq, float r, int64_t* counts,
-                             const int64_t* __restrict__ offsets, int32_t* cand) {
+__global__ void k_candidates(GridDev g, const float* __restrict__ q, const int32_t* __restrict__ qworld, int64_t nq,
+                             float r, int64_t* counts, const int64_t* __restrict__ offsets, int32_t* cand) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nq) return;
   int64_t k = 0;
   const int64_t base = FILL ? offsets[i] : 0;
-  for_each_candidate(g, q[3 * i], q[3 * i + 1], q[3 * i + 2], r, [&](int t) {
+  const int w = qworld ? qworld[i] : 0;
+  for_each_candidate(g, w, q[3 * i], q[3 * i + 1], q[3 * i + 2], r, [&](int t) {
     if (FILL) cand[base + k] = g.perm[t];
     ++k;
   });
@@ -213,11 +230,15 @@ GridDev grid_view(const fs_context* c) {
   g.mask_z = pow2mask(g.dim_z);
   g.inv = c->built_inv;
   g.tile_stats = c->tile_stats;
+  g.worlds = c->worlds;
+  g.nworlds = c->nworlds;
   return g;
 }
 
-int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st) {
+int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st, const int32_t* world) {
   if (n < 0 || (n > 0 && !x) || !(radius > 0.f)) return set_error(FS_ERR_INVALID, "grid_build: bad arguments");
+  if (c->worlds && n > 0 && !world)
+    return set_error(FS_ERR_INVALID, "grid_build: a batched context needs particle_world");
   if (n > c->capacity) return set_error(FS_ERR_CAPACITY, "grid_build: n=%lld > capacity=%lld", (long long)n,
                                         (long long)c->capacity);
   const float inv = 1.0f / radius;
@@ -227,7 +248,10 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
   // a new grid invalidates recorded neighbour lists
   rc = check_cuda(cudaMemsetAsync(c->nb_ctl, 0, sizeof(ListCtl), st), "memset list control");
   if (rc) return rc;
-  if (n > 0)
+  if (n > 0 && c->worlds)
+    k_cell_keys_worlds<<<blocks_for(n), kBlock, 0, st>>>(n, x, world, c->worlds, c->nworlds, inv, c->key, c->slot,
+                                                         c->cell_count, c->status);
+  else if (n > 0)
     k_cell_keys<<<blocks_for(n), kBlock, 0, st>>>(n, x, inv, c->grid.dim_x, c->grid.dim_y, c->grid.dim_z,
                                                    c->grid.rounding, c->key, c->slot, c->cell_count, c->status);
   const int nb = scan_blocks(c->ncell);
@@ -275,6 +299,8 @@ extern "C" {
 const char* fs_last_error_string(void) { return fs::g_err; }
 const char* fs_version(void) { return "fluid_b200 0.1 (sm_100a)"; }
 
+static int context_alloc(fs_context* c, int64_t capacity, int64_t ncell);
+
 int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* grid, int32_t device) {
   if (!out || capacity < 0 || !grid || grid->dim_x <= 0 || grid->dim_y <= 0 || grid->dim_z <= 0 ||
       (grid->rounding != 0 && grid->rounding != 1))
@@ -286,8 +312,72 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
   DeviceGuard dg(device);
   fs_context* c = new fs_context();
   c->device = device;
-  c->capacity = capacity;
   c->grid = *grid;
+  int rc = context_alloc(c, capacity, ncell);
+  if (rc) return rc;
+  *out = c;
+  return FS_OK;
+}
+
+int fs_context_create_worlds(fs_context** out, int64_t capacity, const fs_world_box* worlds, int32_t nworlds,
+                             int32_t device) {
+  if (!out || capacity < 0 || !worlds || nworlds < 1 || nworlds > (1 << 20) || capacity > (int64_t)0x7fffffff)
+    return set_error(FS_ERR_INVALID, "fs_context_create_worlds: bad arguments");
+  WorldDev* host = new WorldDev[nworlds];
+  int64_t ncell = 0;
+  for (int w = 0; w < nworlds; ++w) {
+    const fs_world_box& b = worlds[w];
+    if (b.dims[0] <= 0 || b.dims[1] <= 0 || b.dims[2] <= 0 || !(b.bound_width >= 0.f) || !(b.bound_height >= 0.f) ||
+        !(b.bound_length >= 0.f)) {
+      delete[] host;
+      return set_error(FS_ERR_INVALID, "fs_context_create_worlds: world %d has an empty box or bad walls", w);
+    }
+    const int64_t cells = (int64_t)b.dims[0] * b.dims[1] * b.dims[2];
+    WorldDev& d = host[w];
+    for (int k = 0; k < 3; ++k) {
+      d.clo[k] = b.cell_lo[k];
+      d.dims[k] = b.dims[k];
+    }
+    d.walls[0] = b.bound_width;
+    d.walls[1] = b.bound_height;
+    d.walls[2] = b.bound_length;
+    d.base = (int32_t)(ncell < 0x7fffffff ? ncell : 0x7fffffff);
+    ncell += cells;
+    if (ncell > (int64_t)kScanTile * 4096) {
+      delete[] host;
+      return set_error(FS_ERR_INVALID, "fs_context_create_worlds: more than %lld cells in all",
+                       (long long)kScanTile * 4096);
+    }
+  }
+  DeviceGuard dg(device);
+  fs_context* c = new fs_context();
+  c->device = device;
+  c->grid = fs_grid_config{0, 0, 0, 1};
+  int rc = context_alloc(c, capacity, ncell);  // frees c on failure
+  if (rc) {
+    delete[] host;
+    return rc;
+  }
+  rc = check_cuda(cudaMalloc((void**)&c->worlds, sizeof(WorldDev) * nworlds), "fs_context_create_worlds");
+  if (!rc)
+    rc = check_cuda(cudaMemcpy(c->worlds, host, sizeof(WorldDev) * nworlds, cudaMemcpyHostToDevice),
+                    "fs_context_create_worlds: copy");
+  delete[] host;
+  if (rc) {
+    fs_context_destroy(c);
+    return rc;
+  }
+  c->nworlds = nworlds;
+  *out = c;
+  return FS_OK;
+}
+
+int32_t fs_context_worlds(const fs_context* c) { return c ? c->nworlds : -1; }
+int64_t fs_context_cells(const fs_context* c) { return c ? c->ncell : -1; }
+
+// Device scratch of a context; frees the context on failure.
+static int context_alloc(fs_context* c, int64_t capacity, int64_t ncell) {
+  c->capacity = capacity;
   c->ncell = ncell;
   const int64_t cap = capacity > 0 ? capacity : 1;
   const int nb = scan_blocks(ncell);
@@ -328,7 +418,6 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
     fs_context_destroy(c);
     return rc;
   }
-  *out = c;
   return FS_OK;
 }
 
@@ -340,7 +429,7 @@ int fs_context_destroy(fs_context* c) {
   timer_free(c->timer);
   void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
                 c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
-                c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl};
+                c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete c;
@@ -351,8 +440,17 @@ int64_t fs_context_capacity(const fs_context* c) { return c ? c->capacity : -1; 
 
 int fs_grid_build(fs_context* c, const float* x, int64_t n, float radius, fs_stream_t stream) {
   if (!c) return set_error(FS_ERR_INVALID, "fs_grid_build: null context");
+  if (c->worlds) return set_error(FS_ERR_INVALID, "fs_grid_build: batched context, use fs_grid_build_worlds");
   DeviceGuard dg(c->device);
-  return grid_build(c, x, n, radius, (cudaStream_t)stream);
+  return grid_build(c, x, n, radius, (cudaStream_t)stream, nullptr);
+}
+
+int fs_grid_build_worlds(fs_context* c, const float* x, const int32_t* world, int64_t n, float radius,
+                         fs_stream_t stream) {
+  if (!c) return set_error(FS_ERR_INVALID, "fs_grid_build_worlds: null context");
+  if (!c->worlds) return set_error(FS_ERR_INVALID, "fs_grid_build_worlds: not a batched context");
+  DeviceGuard dg(c->device);
+  return grid_build(c, x, n, radius, (cudaStream_t)stream, world);
 }
 
 int fs_grid_tables(fs_context* c, int32_t* point_ids, int32_t* point_cells, int32_t* cell_starts,
@@ -369,8 +467,24 @@ int fs_grid_tables(fs_context* c, int32_t* point_ids, int32_t* point_cells, int3
   return launch_check("fs_grid_tables");
 }
 
+static int grid_candidates(fs_context* c, const float* q, const int32_t* qworld, int64_t nq, float r,
+                           int64_t* counts, const int64_t* offsets, int32_t* cand, fs_stream_t stream);
+
 int fs_grid_candidates(fs_context* c, const float* q, int64_t nq, float r, int64_t* counts, const int64_t* offsets,
                        int32_t* cand, fs_stream_t stream) {
+  if (c && c->worlds) return set_error(FS_ERR_INVALID, "fs_grid_candidates: batched context, use *_worlds");
+  return grid_candidates(c, q, nullptr, nq, r, counts, offsets, cand, stream);
+}
+
+int fs_grid_candidates_worlds(fs_context* c, const float* q, const int32_t* qworld, int64_t nq, float r,
+                              int64_t* counts, const int64_t* offsets, int32_t* cand, fs_stream_t stream) {
+  if (c && !c->worlds) return set_error(FS_ERR_INVALID, "fs_grid_candidates_worlds: not a batched context");
+  if (nq > 0 && !qworld) return set_error(FS_ERR_INVALID, "fs_grid_candidates_worlds: null qworld");
+  return grid_candidates(c, q, qworld, nq, r, counts, offsets, cand, stream);
+}
+
+static int grid_candidates(fs_context* c, const float* q, const int32_t* qworld, int64_t nq, float r,
+                           int64_t* counts, const int64_t* offsets, int32_t* cand, fs_stream_t stream) {
   if (!c || nq < 0 || (nq > 0 && (!q || !counts)) || (cand && !offsets))
     return set_error(FS_ERR_INVALID, "fs_grid_candidates: bad arguments");
   if (c->built_n < 0) return set_error(FS_ERR_NOGRID, "fs_grid_candidates: no grid built");
@@ -380,12 +494,12 @@ int fs_grid_candidates(fs_context* c, const float* q, int64_t nq, float r, int64
   cudaStream_t st = (cudaStream_t)stream;
   if (cand) {
     PassScope ps_(c, P_OTHER, st);
-    k_candidates<true><<<blocks_for(nq), kBlock, 0, st>>>(g, q, nq, r, counts, offsets, cand);
+    k_candidates<true><<<blocks_for(nq), kBlock, 0, st>>>(g, q, qworld, nq, r, counts, offsets, cand);
   }
   else
     {
       PassScope ps_(c, P_OTHER, st);
-      k_candidates<false><<<blocks_for(nq), kBlock, 0, st>>>(g, q, nq, r, counts, nullptr, nullptr);
+      k_candidates<false><<<blocks_for(nq), kBlock, 0, st>>>(g, q, qworld, nq, r, counts, nullptr, nullptr);
     }
   return launch_check("fs_grid_candidates");
 }

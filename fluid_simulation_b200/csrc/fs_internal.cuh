@@ -42,7 +42,18 @@ struct PassTimer {
   int* pass_of = nullptr;     // pass of each recorded pair
 };
 
+// One world (scene) of a batched context: its own box of cells (no hashing,
+// no aliasing between worlds) and its own walls.
+struct WorldDev {
+  int32_t clo[3];  // cell coordinate of the box's first cell per axis
+  int32_t dims[3]; // cells per axis
+  int32_t base;    // key of its first cell
+  float walls[3];  // bound_width, bound_height, bound_length of its tank
+};
+
 struct GridDev {
+  const WorldDev* worlds = nullptr;  // batched context: per-world boxes (nullptr: the reference hash grid)
+  int32_t nworlds = 0;
   const int32_t* off;   // [ncell + 1] exclusive prefix of cell occupancy (hash-key order)
   const int32_t* perm;  // [n] sorted slot -> original particle index (warp's point_ids)
   const int32_t* skey;  // [n] cell key of each sorted slot (warp's point_cells)
@@ -97,6 +108,11 @@ struct fs_context {
   int32_t* nb_cnt = nullptr;     // [cap]
   void* nb_ctl = nullptr;        // ListCtl
 
+  // batched (multi-world) contexts
+  fs::WorldDev* worlds = nullptr;  // [nworlds] device table
+  int32_t nworlds = 0;
+  float world_cell = 0.f;          // cell width of the world boxes (the solvers' h)
+
   // instrumentation
   fs::PassTimer timer;
   int64_t launches = 0;  // kernels launched through this context (host count)
@@ -148,7 +164,8 @@ struct PassScope {
 };
 
 // grid build (fs_grid.cu)
-int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st);
+// world: particle_world of the model (required by batched contexts, unused otherwise)
+int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st, const int32_t* world);
 GridDev grid_view(const fs_context* c);
 
 // DFSPH residual helper shared with the separate-pass entry (fs_dfsph.cu)
@@ -162,8 +179,12 @@ constexpr float kPi = 3.14159265358979323846f;
 // The .w word of a position: PF bits (a denormal, adds nothing measurable to
 // an r^2) for an active particle, +inf for an inactive one, so that an
 // r^2 + w test rejects inactive candidates without reading any flag.
+// Bits 2..21 carry the world index in batched contexts (still a denormal).
 FS_DEV int pf_of(float4 p) { return __float_as_int(p.w) & (PF_ACTIVE | PF_DYNAMIC); }
-FS_DEV float pack_pf(int pf) { return __int_as_float((pf & PF_ACTIVE) ? pf : 0x7f800000); }
+FS_DEV float pack_pf(int pf, int world = 0) {
+  return __int_as_float((pf & PF_ACTIVE) ? (pf | ((world & 0xFFFFF) << 2)) : 0x7f800000);
+}
+FS_DEV int world_of(float4 p) { return (__float_as_int(p.w) >> 2) & 0xFFFFF; }
 
 // Distance computed with individually rounded operations (no FMA), so that
 // decisions such as `r < h` are bit-identical to a strict FP32 evaluation.
@@ -261,6 +282,61 @@ FS_DEV int phys_cell(const GridDev& g, int x, int y, int z) {
 // f(t) receives the cell-sorted SLOT t (original index = perm[t]).  A run of
 // consecutive x cells is one contiguous slot range because cell offsets are a
 // prefix sum in hash-key order; a run that wraps modulo dim_x splits in two.
+FS_DEV int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Batched contexts.  A world's cell along one axis is the reference's cell
+// coordinate (warp's truncating int(v / cell), as the hash grid bins it)
+// relative to the box's first cell, clamped into the box.  The map is
+// monotone in v, so a query box [p - r, p + r] mapped the same way covers
+// every particle of the world within r of p, including particles outside the
+// box (they sit in its edge cells).  Inside the box the cells, their order
+// and the order inside each cell are those of the hash grid of the world
+// alone (no aliasing while a world spans fewer cells than the hash dims), so
+// a batched step reproduces the step of each world by itself.  No hashing:
+// cells of different worlds never alias, and a query never leaves its world.
+FS_DEV int world_axis_cell(float v, float inv, int clo, int d) {
+  return clampi(to_cell(__fmul_rn(v, inv), 0) - clo, 0, d - 1);
+}
+
+FS_DEV int world_index(int w, int nworlds) { return clampi(w, 0, nworlds - 1); }
+
+FS_DEV int world_cell_key(const WorldDev& W, float inv, float px, float py, float pz) {
+  const int cx = world_axis_cell(px, inv, W.clo[0], W.dims[0]);
+  const int cy = world_axis_cell(py, inv, W.clo[1], W.dims[1]);
+  const int cz = world_axis_cell(pz, inv, W.clo[2], W.dims[2]);
+  return W.base + (cz * W.dims[1] + cy) * W.dims[0] + cx;
+}
+
+// The query cells of world w in the order z-outer, y, x-inner; each row of
+// x cells is one contiguous slot range.
+template <class F>
+FS_DEV void for_each_candidate_world(const GridDev& g, int w, float px, float py, float pz, float r, F&& f) {
+  const WorldDev& W = g.worlds[world_index(w, g.nworlds)];
+  auto cell = [&](float v, int k) { return world_axis_cell(v, g.inv, W.clo[k], W.dims[k]); };
+  const int x0 = cell(__fsub_rn(px, r), 0), x1 = cell(__fadd_rn(px, r), 0);
+  const int y0 = cell(__fsub_rn(py, r), 1), y1 = cell(__fadd_rn(py, r), 1);
+  const int z0 = cell(__fsub_rn(pz, r), 2), z1 = cell(__fadd_rn(pz, r), 2);
+  for (int z = z0; z <= z1; ++z)
+    for (int y = y0; y <= y1; ++y) {
+      const int row = W.base + (z * W.dims[1] + y) * W.dims[0];
+      const int e = __ldg(g.off + row + x1 + 1);
+      for (int t = __ldg(g.off + row + x0); t < e; ++t) f(t);
+    }
+}
+
+template <class F>
+FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f);
+
+// The candidates of a query at (px, py, pz) of world w (w is ignored by the
+// reference hash grid).
+template <class F>
+FS_DEV void for_each_candidate(const GridDev& g, int w, float px, float py, float pz, float r, F&& f) {
+  if (g.worlds)
+    for_each_candidate_world(g, w, px, py, pz, r, f);
+  else
+    for_each_candidate(g, px, py, pz, r, f);
+}
+
 template <class F>
 FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f) {
   const int x0 = to_cell(__fmul_rn(__fsub_rn(px, r), g.inv), g.rounding);
@@ -302,12 +378,14 @@ FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, f
 //   mode 1: DFSPH  (solver_dfsph.py:407-442) same walls, damping unconditional
 //   mode 2: PBF    (solver_pbf.py:467-517)  walls inset by radius + eps, damp outward v
 struct Walls {
-  float xmin, xmax, ymin, ymax, zmin, zmax, damping;
+  float xmin, xmax, ymin, ymax, zmin, zmax, damping, radius, eps;
   int mode;
 };
 
-inline Walls make_walls(float w, float hgt, float l, float damping, int mode, float radius, float eps) {
+__host__ __device__ inline Walls make_walls(float w, float hgt, float l, float damping, int mode, float radius, float eps) {
   Walls b;
+  b.radius = radius;
+  b.eps = eps;
   b.mode = mode;
   b.damping = damping;
   if (mode == 2) {
@@ -326,6 +404,13 @@ inline Walls make_walls(float w, float hgt, float l, float damping, int mode, fl
     b.zmax = l * 2.0f;
   }
   return b;
+}
+
+// The walls of world w in a batched context (its tank), else the step's walls.
+FS_DEV Walls walls_of(const Walls& b, const GridDev& g, int w) {
+  if (!g.worlds) return b;
+  const WorldDev& W = g.worlds[world_index(w, g.nworlds)];
+  return make_walls(W.walls[0], W.walls[1], W.walls[2], b.damping, b.mode, b.radius, b.eps);
 }
 
 FS_DEV void apply_walls(const Walls& b, float3& p, float3& v) {
@@ -360,6 +445,12 @@ FS_DEV int particle_pf(const int32_t* flags, const int32_t* mask, int64_t i) {
   const bool act = (flags[i] & 1) != 0;
   const bool dyn = act && (mask ? mask[i] == 0 : true);
   return (act ? PF_ACTIVE : 0) | (dyn ? PF_DYNAMIC : 0);
+}
+
+// walls_of for a kernel in original particle order (world from particle_world)
+FS_DEV Walls walls_of_particle(const Walls& b, const GridDev& g, const fs_model& m, int64_t i) {
+  if (!g.worlds) return b;
+  return walls_of(b, g, m.particle_world ? m.particle_world[i] : 0);
 }
 
 FS_DEV float3 gravity_of(const fs_model& m, int64_t i) {

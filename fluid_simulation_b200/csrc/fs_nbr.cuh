@@ -113,7 +113,7 @@ template <bool COUNT>
 FS_DEV int record_list(const GridDev& g, const float4* __restrict__ xs, int s, float4 xi, float h, float h2m,
                        const NbrList& L) {
   int n = 0, ncand = 0;
-  for_each_candidate(g, xi.x, xi.y, xi.z, h, [&](int t) {
+  for_each_candidate(g, world_of(xi), xi.x, xi.y, xi.z, h, [&](int t) {
     const float4 xj = __ldg(xs + t);
     if (COUNT) ncand += (t != s) ? (__float_as_int(xj.w) & PF_ACTIVE) : 0;
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -131,7 +131,7 @@ FS_DEV int record_list(const GridDev& g, const float4* __restrict__ xs, int s, f
 template <bool WITH_SELF, class Pair>
 FS_DEV void scan_grid(const GridDev& g, const float4* __restrict__ xs, int s, float4 xi, float h, float h2m,
                       Pair&& pair) {
-  for_each_candidate(g, xi.x, xi.y, xi.z, h, [&](int t) {
+  for_each_candidate(g, world_of(xi), xi.x, xi.y, xi.z, h, [&](int t) {
     const float4 xj = __ldg(xs + t);
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
     if (fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xj.w))) <= h2m && (WITH_SELF || t != s)) pair(t, xj);

@@ -19,22 +19,22 @@ namespace fs {
 
 __global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
                                 const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
-                                float* __restrict__ mv, uint32_t* status);
+                                float* __restrict__ mv, uint32_t* status, int nworlds);
 
 namespace {
 
 // predict_velocity_with_gravity (193-208) + predict_positions (212-224) +
 // apply_position_bounds (367-399); original order.
-__global__ void k_predict(int64_t n, fs_model m, const float* __restrict__ x, const float* __restrict__ v, float dt,
-                          Walls walls, float* __restrict__ x_pred, float* __restrict__ v_pred) {
+__global__ void k_predict(int64_t n, fs_model m, GridDev g, const float* __restrict__ x, const float* __restrict__ v,
+                          float dt, Walls walls, float* __restrict__ x_pred, float* __restrict__ v_pred) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float3 p = ld3(x, i), u = ld3(v, i);
   if (particle_pf(m.particle_flags, m.particle_mask, i) & PF_DYNAMIC) {
-    const float3 g = gravity_of(m, i);
-    u = make_float3(u.x + dt * g.x, u.y + dt * g.y, u.z + dt * g.z);
+    const float3 gv = gravity_of(m, i);
+    u = make_float3(u.x + dt * gv.x, u.y + dt * gv.y, u.z + dt * gv.z);
     p = make_float3(p.x + dt * u.x, p.y + dt * u.y, p.z + dt * u.z);
-    clamp_position(walls, p);
+    clamp_position(walls_of_particle(walls, g, m, i), p);
   }
   st3(x_pred, i, p);
   st3(v_pred, i, u);
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kNbBlock) k_accel_apply(AccelArgs a) {
   st3(a.accel, i, make_float3(ax, ay, az));
   const float dvx = a.dt * ax, dvy = a.dt * ay, dvz = a.dt * az;
   float3 p = make_float3(xi.x + a.dt * dvx, xi.y + a.dt * dvy, xi.z + a.dt * dvz);
-  clamp_position(a.walls, p);
+  clamp_position(walls_of(a.walls, a.g, world_of(xi)), p);
   a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
 }
 
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kNbBlock) k_delta(DeltaArgs a) {
   st3(a.delta_p, i, d);
   if (a.xs_out) {
     float3 p = make_float3(xi.x + d.x, xi.y + d.y, xi.z + d.z);
-    if (a.clamp) clamp_position(a.walls, p);
+    if (a.clamp) clamp_position(walls_of(a.walls, a.g, world_of(xi)), p);
     a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
   }
 }
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kNbBlock) k_xsph_final(XsphArgs a) {
       });
       v = make_float3(fmaf(a.c, cx, vi.x), fmaf(a.c, cy, vi.y), fmaf(a.c, cz, vi.z));
     }
-    if (a.bounds) apply_walls(a.walls, p, v);
+    if (a.bounds) apply_walls(walls_of(a.walls, a.g, world_of(xi)), p, v);
   }
   if (a.x_out) st3(a.x_out, i, p);
   st3(a.v_out, i, v);
@@ -364,7 +364,7 @@ int gather_pbf(fs_context* c, const fs_model* m, const float* x_in, cudaStream_t
   {
     PassScope ps_(c, P_GATHER, st);
     k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, c->xo_tmp, c->vo_tmp, c->xs, c->vs, c->mv,
-                                                    c->status);
+                                                    c->status, c->nworlds);
   }
   {
     PassScope ps_(c, P_GATHER, st);
@@ -400,10 +400,11 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   int rc;
   {
     PassScope ps_(c, P_PBF_PREDICT, st);
-    k_predict<<<blocks_for(n), kBlock, 0, st>>>(n, *m, si->particle_q, si->particle_qd, dt, w, c->xo_tmp, c->vo_tmp);
+    k_predict<<<blocks_for(n), kBlock, 0, st>>>(n, *m, grid_view(c), si->particle_q, si->particle_qd, dt, w, c->xo_tmp,
+                                                c->vo_tmp);
   }
   if ((rc = launch_check("pbf predict"))) return rc;
-  if ((rc = grid_build(c, c->xo_tmp, n, h, st))) return rc;
+  if ((rc = grid_build(c, c->xo_tmp, n, h, st, m->particle_world))) return rc;
   if ((rc = gather_pbf(c, m, si->particle_q, st))) return rc;
   const GridDev g = grid_view(c);
   // neighbour lists: density -> accel, lambda -> delta, final density -> XSPH
@@ -488,7 +489,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
         PassScope ps_(c, P_GATHER, st);
         k_scatter_x<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, cur, c->xo_tmp);
       }
-      if ((rc = grid_build(c, c->xo_tmp, n, h, st))) return rc;
+      if ((rc = grid_build(c, c->xo_tmp, n, h, st, m->particle_world))) return rc;
       if ((rc = gather_pbf(c, m, si->particle_q, st))) return rc;
       cur = c->xs;
       nxt = c->xs2;
@@ -534,7 +535,7 @@ int fs_pbf_density(fs_context* c, const fs_model* m, const float* x, float h, fl
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, x, c->xs, c->vs, c->mv,
-                                                       c->status);
+                                                       c->status, c->nworlds);
   k_density<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(grid_view(c), nbr_list(c), 0, m->n, c->xs, c->vs, c->mv, h,
                                                                 rho, c->sc2);
   return launch_check("fs_pbf_density");
@@ -548,7 +549,7 @@ int fs_pbf_lambda(fs_context* c, const fs_model* m, const float* x_pred, const f
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, x_pred, c->xs, c->vs, nullptr,
-                                                       c->status);
+                                                       c->status, c->nworlds);
   LambdaArgs la;
   la.g = grid_view(c);
   la.L = nbr_list(c);
@@ -577,7 +578,7 @@ int fs_pbf_delta(fs_context* c, const fs_model* m, const float* x_pred, const fl
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, x_pred, c->xs, c->vs, nullptr,
-                                                       c->status);
+                                                       c->status, c->nworlds);
   k_gather_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, pbf_lambda, c->sc1);
   DeltaArgs da;
   da.g = grid_view(c);
@@ -609,7 +610,7 @@ int fs_pbf_xsph(fs_context* c, const fs_model* m, const float* x_pred, const flo
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, v_in, c->xs, c->vs2, nullptr,
-                                                       c->status);
+                                                       c->status, c->nworlds);
   k_gather_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, rho, c->sc1);
   k_rho_ratio<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->sc1, c->vs2, c->sc2);
   XsphArgs xa;

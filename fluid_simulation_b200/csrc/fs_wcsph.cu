@@ -18,13 +18,15 @@ namespace fs {
 // solver_wcsph.py:110-116).
 __global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
                                 const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
-                                float* __restrict__ mv, uint32_t* status) {
+                                float* __restrict__ mv, uint32_t* status, int nworlds) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const int32_t i = perm[s];
   const float3 p = ld3(x, i);
   const int pf = particle_pf(m.particle_flags, m.particle_mask, i);
-  xs[s] = make_float4(p.x, p.y, p.z, pack_pf(pf));
+  // batched contexts carry the world in the flags word (queries stay in it)
+  const int w = (nworlds > 0 && m.particle_world) ? world_index(m.particle_world[i], nworlds) : 0;
+  xs[s] = make_float4(p.x, p.y, p.z, pack_pf(pf, w));
   const float mass = m.particle_mass[i];
   if (vs) {
     const float3 u = ld3(v, i);
@@ -155,18 +157,9 @@ __global__ void __launch_bounds__(kNbBlock) k_wcsph_force(ForceArgs a) {
   st3(a.accel, i, acc);
   float3 v = make_float3(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z);
   float3 p = make_float3(xi.x + v.x * a.dt, xi.y + v.y * a.dt, xi.z + v.z * a.dt);
-  apply_walls(a.walls, p, v);
+  apply_walls(walls_of(a.walls, a.g, world_of(xi)), p, v);
   st3(a.v_out, i, v);
   st3(a.x_out, i, p);
-}
-
-// (a[i], b[i]) of original order into cell order
-__global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
-                              const float* __restrict__ b, float2* __restrict__ out) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const int32_t i = perm[s];
-  out[s] = make_float2(a[i], b ? b[i] : 0.f);
 }
 
 // (rho, p) of original order -> force-pass ratios in cell order
@@ -183,7 +176,7 @@ int wcsph_gather(fs_context* c, const fs_model* m, const float* x, const float* 
   const int64_t n = m->n;
   {
     PassScope ps_(c, P_GATHER, st);
-    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, x, v, c->xs, c->vs, c->mv, c->status);
+    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, x, v, c->xs, c->vs, c->mv, c->status, c->nworlds);
   }
   return launch_check("wcsph gather");
 }
@@ -265,7 +258,7 @@ int fs_wcsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   const float h = p->smoothing_length;
-  if ((rc = grid_build(c, si->particle_q, m->n, h, st))) return rc;
+  if ((rc = grid_build(c, si->particle_q, m->n, h, st, m->particle_world))) return rc;
   if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
   if ((rc = launch_density(c, m, h, p->clamp_negative_pressure, true, so->rho, so->pressure, st))) return rc;
   return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st, true);
@@ -280,7 +273,7 @@ int fs_wcsph_density(fs_context* c, const fs_model* m, const float* x, float h, 
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, nullptr, c->xs, nullptr, c->mv,
-                                                       c->status);
+                                                       c->status, c->nworlds);
   return launch_density(c, m, h, clamp_negative, true, rho, pressure, st);
 }
 
@@ -294,7 +287,7 @@ int fs_wcsph_force_integrate(fs_context* c, const fs_model* m, const fs_state* s
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
-  k_gather_pair<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, so->rho, so->pressure, c->sc2);
+  k_gather_ratios<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, so->rho, so->pressure, c->sc2);
   if ((rc = launch_check("wcsph gather rho/p"))) return rc;
   return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st, false);
 }

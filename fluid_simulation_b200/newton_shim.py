@@ -351,6 +351,92 @@ class HashGrid:
             pass
 
 
+class WorldGrid(HashGrid):
+    """Segmented grid of a batched model: one box of cells per world
+    (``Model.particle_world``), keyed (world, cell), and one tank of walls
+    per world.  Drop it in as ``model.particle_grid`` and the WCSPH / PBF
+    solvers advance every world in one launch per pass; the walls of each
+    world replace the solver config's ``bound_*``.
+
+    ``boxes``: one ``(cell_lo[3], dims[3], (bound_width, bound_height,
+    bound_length))`` per world: the box covers the cells whose coordinate
+    ``int(x / h)`` (truncating, as the reference's hash grid) lies in
+    ``[cell_lo, cell_lo + dims)``, h = the solver's smoothing length."""
+
+    def __init__(self, boxes, device="cuda:0"):
+        super().__init__(1, 1, 1, device=device, rounding=1)
+        self.boxes = [(tuple(map(int, lo)), tuple(map(int, dims)), tuple(map(float, walls)))
+                      for lo, dims, walls in boxes]
+        if not self.boxes:
+            raise ValueError("WorldGrid needs at least one world")
+        self.num_cells = sum(d[0] * d[1] * d[2] for _, d, _ in self.boxes)
+
+    @property
+    def num_worlds(self) -> int:
+        return len(self.boxes)
+
+    def _world_boxes(self):
+        arr = (_lib.WorldBox * len(self.boxes))()
+        for k, (lo, dims, walls) in enumerate(self.boxes):
+            arr[k].cell_lo[:] = lo
+            arr[k].dims[:] = dims
+            arr[k].bound_width, arr[k].bound_height, arr[k].bound_length = walls
+        return arr
+
+    def reserve(self, num_points: int) -> None:
+        num_points = int(num_points)
+        if self._ctx.value and num_points <= self.capacity:
+            return
+        lib = _lib.load()
+        self._destroy()
+        dev = self.device.index if self.device.index is not None else torch.cuda.current_device()
+        boxes = self._world_boxes()
+        _lib.check(lib.fs_context_create_worlds(C.byref(self._ctx), num_points, boxes, len(self.boxes), dev),
+                   "WorldGrid.reserve")
+        self.capacity = num_points
+
+    def build(self, points: torch.Tensor, radius: float, world: torch.Tensor = None) -> None:
+        if world is None:
+            raise ValueError("WorldGrid.build needs the particle_world array")
+        n = int(points.shape[0])
+        if n > self.capacity:
+            self.reserve(n)
+        pts = points.contiguous()
+        w = world.to(torch.int32).contiguous()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(_lib.load().fs_grid_build_worlds(self._ctx, pts.data_ptr(), w.data_ptr(), n, float(radius), stream),
+                   "WorldGrid.build")
+        self.num_points = n
+
+    def tables(self):
+        n = self.num_points
+        nc = self.num_cells
+        t = [torch.empty(k, dtype=torch.int32, device=self.device) for k in (n, n, nc, nc)]
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(_lib.load().fs_grid_tables(self._ctx, *[x.data_ptr() for x in t], stream), "WorldGrid.tables")
+        return tuple(t)
+
+    def candidates(self, queries: torch.Tensor, radius: float, qworld: torch.Tensor = None):
+        if qworld is None:
+            raise ValueError("WorldGrid.candidates needs the world of each query")
+        q = queries.contiguous()
+        qw = qworld.to(torch.int32).contiguous()
+        nq = q.shape[0]
+        lib = _lib.load()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        counts = torch.empty(nq, dtype=torch.int64, device=self.device)
+        _lib.check(lib.fs_grid_candidates_worlds(self._ctx, q.data_ptr(), qw.data_ptr(), nq, float(radius),
+                                                 counts.data_ptr(), None, None, stream), "WorldGrid.candidates")
+        offsets = torch.zeros(nq + 1, dtype=torch.int64, device=self.device)
+        offsets[1:] = torch.cumsum(counts, 0)
+        total = int(offsets[-1])
+        cand = torch.empty(max(total, 1), dtype=torch.int32, device=self.device)
+        _lib.check(lib.fs_grid_candidates_worlds(self._ctx, q.data_ptr(), qw.data_ptr(), nq, float(radius),
+                                                 counts.data_ptr(), offsets.data_ptr(), cand.data_ptr(), stream),
+                   "WorldGrid.candidates")
+        return offsets, cand[:total]
+
+
 class SolverBase:
     def __init__(self, model: Model):
         self.model = model

@@ -152,6 +152,40 @@ int fs_grid_tables(fs_context* ctx, int32_t* point_ids, int32_t* point_cells, in
 int fs_grid_candidates(fs_context* ctx, const float* q, int64_t nq, float r, int64_t* counts,
                        const int64_t* offsets, int32_t* cand, fs_stream_t stream);
 
+/* ---- batched worlds (no counterpart in the reference) ------------------
+ * Many independent scenes (Newton worlds, Model.particle_world) advance in
+ * one model: one launch per pass covers every scene.  The reference puts all
+ * worlds of a model into one hash grid, so scenes that overlap in space
+ * would interact; a batched context instead gives each world its own box of
+ * cells keyed (world, cell): per axis cell = clamp(c - cell_lo, 0, dims - 1)
+ * with c the reference's truncating cell coordinate int(x / h), no hashing,
+ * and a query never leaves its world.  Inside its box a world sees the cells,
+ * candidate order and results of the hash grid of that world alone.  Each
+ * world also
+ * has its own tank: the walls of the step parameters are replaced by
+ * fs_world_box.bound_* of the particle's world.  particle_world is required;
+ * an index outside [0, nworlds) is clamped and raises FS_STATUS_BOUNDS.
+ * WCSPH and PBF substeps and every separate pass accept a batched context;
+ * fs_dfsph_substep, whose iteration decisions are global, returns
+ * FS_ERR_INVALID.  fs_grid_build / fs_grid_candidates on a batched context
+ * (and the *_worlds forms on a hash-grid context) return FS_ERR_INVALID. */
+typedef struct {
+  int32_t cell_lo[3];  /* cell coordinate int(x / h) of the box's first cell per axis */
+  int32_t dims[3];     /* cells per axis */
+  float bound_width, bound_height, bound_length;  /* tank [-W,W]x[-H,H]x[0,2L] */
+} fs_world_box;
+
+int fs_context_create_worlds(fs_context** out, int64_t capacity, const fs_world_box* worlds, int32_t nworlds,
+                             int32_t device);
+int32_t fs_context_worlds(const fs_context* ctx); /* 0 for a hash-grid context */
+int64_t fs_context_cells(const fs_context* ctx);  /* cells of the grid (the size of cell_starts) */
+/* grid.build for a batched context: world[n] = Model.particle_world. */
+int fs_grid_build_worlds(fs_context* ctx, const float* x, const int32_t* world, int64_t n, float radius,
+                         fs_stream_t stream);
+/* fs_grid_candidates of queries that belong to world qworld[i]. */
+int fs_grid_candidates_worlds(fs_context* ctx, const float* q, const int32_t* qworld, int64_t nq, float r,
+                              int64_t* counts, const int64_t* offsets, int32_t* cand, fs_stream_t stream);
+
 /* ---- whole substeps --------------------------------------------------- */
 /* SolverWCSPH.step (solver_wcsph.py:431-535).  accel = solver._particle_accel [n][3]. */
 int fs_wcsph_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
