@@ -150,6 +150,111 @@ def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1):
                        f"(C++ restatement of the reference solver, OpenMP, {cores} threads)")
 
 
+# ------------------------------------------------------ batched scenes ----
+def batched_configs(batch, kind):
+    """Solver config and dt of a batch of dam-break scenes: the reference
+    harness's PBF config (4 iterations, ...) at dt = 1/240, or WCSPH at the
+    acoustic limit 0.25 h / c0 of the stiffest scene.  Walls come from each
+    scene (the config's bound_* apply only to the plain per-scene runs)."""
+    from fluid_simulation_b200.solver import SolverPBF, SolverWCSPH
+    common = dict(particle_radius=batch.radius, particle_length=batch.spacing, smoothing_length_coff=2.0,
+                  boundary_damping=0.0)
+    if kind == "pbf":
+        return SolverPBF, (lambda walls: SolverPBF.PbfConfig(
+            max_iterations=4, lambda_epsilon=100.0, min_neighbors_for_lambda=8, scorr_k=0.0,
+            max_delta_position=batch.radius * 0.5, xsph_c=0.05, bound_width=walls[0], bound_height=walls[1],
+            bound_length=walls[2], **common)), 1.0 / 240.0, 4
+    c0 = (max(s.stiffness for s in batch.scenes) * 7.0 / 1000.0) ** 0.5
+    return SolverWCSPH, (lambda walls: SolverWCSPH.SphConfig(
+        bound_width=walls[0], bound_height=walls[1], bound_length=walls[2], **common)), 0.25 * batch.h / c0, 8
+
+
+def time_batched(kind, dev, flush, frames=2, warm=1):
+    """All scenes of make_batch() (256 dam-break scenes, ~6.2 M particles)
+    advanced as one batched model, a frame of substeps replayed from one CUDA
+    graph, against the same scenes run one by one with the plain solver
+    (eagerly, and with one frame graph per scene).  Both start from the same
+    state and run the same frames; their final states are compared bit for
+    bit (equal error: the batched step reproduces each scene's plain step)."""
+    import torch
+    from fluid_simulation_b200 import _lib
+    from fluid_simulation_b200.batch import batched_model, make_batch, scene_model
+    from fluid_simulation_b200.graph import FrameGraph
+    lib = _lib.load()
+    b = make_batch()
+    cls, cfg_of, dt, sub = batched_configs(b, kind)
+    n = b.total
+
+    def timed(run, nframes):
+        tot = 0.0
+        for _ in range(nframes):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run()
+            e1.record()
+            flush.zero_()
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot
+
+    # batched: one model, one graph per frame
+    mb = batched_model(b, cls, device=dev)
+    sb = cls(mb, cfg_of((1.0, 1.0, 1.0)))
+    ctx_b = mb.particle_grid._ctx
+    l0 = lib.fs_launch_count(ctx_b)
+    fb = FrameGraph(sb, mb.state(), mb.state(), dt, substeps=sub, warmup=False)
+    launches_b = lib.fs_launch_count(ctx_b) - l0   # kernels recorded in the frame graph
+    timed(fb.replay, warm)
+    t_batched = timed(fb.replay, frames)
+    # serial: the same scenes, one plain model and solver each
+    scenes = []
+    for k, s in enumerate(b.scenes):
+        m = scene_model(b, k, cls, device=dev)
+        scenes.append((m, cls(m, cfg_of(s.walls)), m.state(), m.state()))
+
+    def serial_frame():
+        for i, (m, sv, a, c) in enumerate(scenes):
+            for _ in range(sub):
+                sv.step(a, c, None, None, dt)
+                a, c = c, a
+            scenes[i] = (m, sv, a, c)
+
+    timed(serial_frame, warm)
+    l0 = sum(lib.fs_launch_count(m.particle_grid._ctx) for m, *_ in scenes)
+    t_serial = timed(serial_frame, frames)
+    launches_s = sum(lib.fs_launch_count(m.particle_grid._ctx) for m, *_ in scenes) - l0
+    graphs = [FrameGraph(sv, a, c, dt, substeps=sub, warmup=False) for m, sv, a, c in scenes]
+
+    def serial_graphs():
+        for g in graphs:
+            g.replay()
+
+    timed(serial_graphs, warm)
+    t_serial_g = timed(serial_graphs, frames)
+    # same number of frames on both sides: batched runs as many as the serial side ran
+    for _ in range(warm + frames):
+        fb.replay()
+    torch.cuda.synchronize()
+    xb = fb.result.particle_q
+    same = all(torch.equal(xb[int(b.starts[k]):int(b.starts[k + 1])], g.result.particle_q)
+               for k, g in enumerate(graphs))
+    rate = lambda ms: round(n * sub * frames / (ms * 1e-3), 1)
+    rec = dict(workload=f"batched_{kind}_256", solver=kind.upper(), scenes=len(b.scenes), particles=n,
+               scene_counts="log-uniform [2000, 100000], seed 3; column fraction U(0.2, 0.6); stiffness and "
+                            "viscosity x U(0.8, 1.2)", spacing=b.spacing, dt=dt, substeps_per_frame=sub,
+               frames=frames, value=rate(t_batched), unit="particle-steps/s",
+               ms_per_frame=round(t_batched / frames, 3), launches_per_frame_batched=int(launches_b),
+               serial_eager=dict(value=rate(t_serial), ms_per_frame=round(t_serial / frames, 3),
+                                 launches_per_frame=launches_s // frames),
+               serial_graph=dict(value=rate(t_serial_g), ms_per_frame=round(t_serial_g / frames, 3)),
+               speedup_vs_serial_eager=round(t_serial / t_batched, 2),
+               speedup_vs_serial_graph=round(t_serial_g / t_batched, 2),
+               final_state_bit_identical_to_serial=bool(same))
+    del fb, graphs, scenes, mb, sb
+    torch.cuda.empty_cache()
+    return rec
+
+
 # --------------------------------------------------------------- clocks ----
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -337,6 +442,10 @@ def run_ours(args):
             del m2, s2, x0, x1
             torch.cuda.empty_cache()
 
+    if world == 1 and not args.no_secondary and not args.no_batched:
+        for kind in ("pbf", "wcsph"):
+            secondary[f"batched_{kind}_256"] = time_batched(kind, dev, flush)
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline and not args.workload.startswith("wcsph_stress"):
         cpu = time_cpu_baseline(args.workload, max_seconds=args.cpu_seconds)
@@ -409,6 +518,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
