@@ -91,6 +91,8 @@ SIGNATURES = {
     "fs_context_cells": (I64, [P]),
     "fs_grid_build_worlds": (C.c_int, [P, P, P, I64, F, P]),
     "fs_grid_candidates_worlds": (C.c_int, [P, P, P, I64, F, P, P, P, P]),
+    "fs_wcsph_substep_adjoint": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), P, P, P, P, P, P, P, P, P, P,
+                                           C.POINTER(WcsphParams), P]),
     "fs_wcsph_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
                                    C.POINTER(WcsphParams), P, P]),
     "fs_dfsph_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),

@@ -199,6 +199,23 @@ int fs_dfsph_info_read(fs_context* ctx, fs_dfsph_info* info); /* synchronises th
 int fs_pbf_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
                    const fs_pbf_params* params, float* accel, float* x_pred, fs_stream_t stream);
 
+/* ---- WCSPH adjoint (no counterpart in the reference, which differentiates
+ * nothing; the reference project's archive took gradients through Warp's
+ * tape) ----------------------------------------------------------------
+ * Reverse-mode derivative of one fs_wcsph_substep with the step's neighbour
+ * set held fixed.  Inputs: the step's input state (particle_q/qd of
+ * state_in), what the forward step wrote (rho, pressure: state_out.sph; accel),
+ * and the adjoints of its outputs (adj_x_out = dL/d particle_q out, adj_v_out =
+ * dL/d particle_qd out, [n][3]).  Writes adj_x_in / adj_v_in (dL/d particle_q
+ * and particle_qd in, [n][3]) and ADDS dL/d stiffness, viscosity and
+ * rest_density per particle into adj_stiffness / adj_viscosity /
+ * adj_rest_density (each may be NULL).  Builds the grid of state_in itself;
+ * uses the context's scratch like a substep. */
+int fs_wcsph_substep_adjoint(fs_context* ctx, const fs_model* model, const fs_state* state_in, const float* rho,
+                             const float* pressure, const float* accel, const float* adj_x_out, const float* adj_v_out,
+                             float* adj_x_in, float* adj_v_in, float* adj_stiffness, float* adj_viscosity,
+                             float* adj_rest_density, const fs_wcsph_params* params, fs_stream_t stream);
+
 /* ---- separate passes (each needs fs_grid_build(positions, h) first) --------
  * WCSPH compute_density_pressure (solver_wcsph.py:120-158). */
 int fs_wcsph_density(fs_context* ctx, const fs_model* model, const float* x, float h, int32_t clamp_negative,

@@ -1,0 +1,55 @@
+"""Shared setup of the WCSPH gradient tests: a small compressed block against
+a wall (pressure, walls and cohesion all active) and the oracle-form model."""
+
+import numpy as np
+import torch
+
+import wcsph_tape
+
+SPACING = 0.01
+H = 2.0 * SPACING
+MASS = 1000.0 * SPACING ** 3
+CFG = dict(particle_radius=0.5 * SPACING, particle_length=SPACING, smoothing_length_coff=2.0, bound_width=0.1,
+           bound_height=0.1, bound_length=0.1, boundary_damping=-0.5, clamp_negative_pressure=True)
+GRAVITY = (0.0, 0.0, -10.0)
+DT = 1.0e-4
+
+
+def block(side=11, squeeze=0.94, seed=0, sigma=0.3):
+    """side^3 particles squeezed to 94 % of the spacing, resting on the floor
+    and touching the -x wall; velocities N(0, sigma)."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(side) * SPACING * squeeze
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    x = x + rng.uniform(-0.03, 0.03, x.shape) * SPACING
+    x = x + np.array([-CFG["bound_width"] + 0.1 * SPACING, -0.5 * g[-1], 0.1 * SPACING])
+    v = rng.normal(size=x.shape) * sigma
+    return x.astype(np.float32), v.astype(np.float32)
+
+
+def params(n, seed=1):
+    rng = np.random.default_rng(seed)
+    return dict(stiffness=(2.5e5 * rng.uniform(0.8, 1.2, n)).astype(np.float32),
+                viscosity=(2e-3 * rng.uniform(0.8, 1.2, n)).astype(np.float32),
+                rest_density=(1000.0 * rng.uniform(0.98, 1.02, n)).astype(np.float32),
+                surface_tension=np.full(n, 0.02, np.float32), exponent=np.full(n, 7.0, np.float32))
+
+
+def oracle_model(x, prm):
+    n = len(x)
+    return dict(particle_flags=np.ones(n, np.int32), particle_mass=np.full(n, MASS, np.float32),
+                particle_world=np.zeros(n, np.int32), gravity=np.array([GRAVITY], np.float32),
+                particle_max_radius=CFG["particle_radius"],
+                sph=dict(particle_mask=np.zeros(n, np.int32), **prm))
+
+
+def tape_rollout(x, v, prm, steps, dt=DT):
+    """FP64 torch rollout; x, v, prm entries are float64 tensors (leaves)."""
+    n = x.shape[0]
+    mass = torch.full((n,), float(np.float32(MASS)), dtype=torch.float64)  # the model stores float32 masses
+    g = torch.tensor(GRAVITY, dtype=torch.float64)
+    cfg = dict(CFG, h=H)
+    for _ in range(steps):
+        x, v = wcsph_tape.substep(x, v, mass, prm["stiffness"], prm["viscosity"], prm["rest_density"],
+                                  prm["exponent"], prm["surface_tension"], g, cfg, dt)
+    return x, v
