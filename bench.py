@@ -255,6 +255,105 @@ def time_batched(kind, dev, flush, frames=2, warm=1):
     return rec
 
 
+# ------------------------------------------------------------- adjoint ----
+def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
+    """Differentiable WCSPH: forward of ``steps`` substeps (the plain drop-in
+    step) against forward + backward through DiffWCSPH (checkpoint every k
+    substeps, segments replayed in the backward).  Loss: mean squared distance
+    of the final positions to the initial ones moved by +0.3 m in x;
+    gradients w.r.t. v0 [N, 3], stiffness, viscosity and rest density.
+    Workload: make_scene(50000) (50,232 particles) or, batched, the 256 scenes
+    of make_batch() as one model."""
+    import torch
+    from fluid_simulation_b200.batch import batched_model, make_batch
+    from fluid_simulation_b200.dam_break import material, solver_config
+    from fluid_simulation_b200.diff import DiffWCSPH
+    from fluid_simulation_b200.graph import FrameGraph
+    from fluid_simulation_b200.newton_shim import model_from_arrays
+    from fluid_simulation_b200.scene import make_scene
+    from fluid_simulation_b200.solver import SolverWCSPH
+    if batched:
+        b = make_batch()
+        _, cfg_of, dt, _ = batched_configs(b, "wcsph")
+        model = batched_model(b, SolverWCSPH, device=dev)
+        cfg = cfg_of((1.0, 1.0, 1.0))
+        stiff = torch.as_tensor(b.per_particle("stiffness"), device=dev)
+        visc = torch.as_tensor(b.per_particle("viscosity"), device=dev)
+        rest = torch.full_like(stiff, 1000.0)
+        desc = dict(workload="batched_adjoint_wcsph_256", scenes=len(b.scenes), particles=b.total)
+    else:
+        s = make_scene(50000)
+        attrs = dict(material("wcsph", s), particle_mask=0)
+        model = model_from_arrays(s.positions, np.zeros_like(s.positions), s.mass, device=dev, radius=s.radius,
+                                  gravity=(s.spec.gravity,), attributes=attrs, solver_cls=SolverWCSPH)
+        cfg = solver_config("wcsph", s)
+        dt = 0.25 * 2.0 * s.spacing / (2.5e5 * 7.0 / 1000.0) ** 0.5
+        stiff, visc, rest = (torch.tensor(v, device=dev) for v in (2.5e5, 1.0e-6, 1000.0))
+        desc = dict(workload="adjoint_wcsph_50232", scene="make_scene(50000) dam break", particles=s.count)
+    n = model.particle_count
+    x0 = model.particle_q.clone()
+    target = x0 + torch.tensor([0.3, 0.0, 0.0], device=dev)
+    sim = DiffWCSPH(model, cfg, dt, checkpoint_every=k)
+    sim_replay = DiffWCSPH(model, cfg, dt, checkpoint_every=k, record_bytes=0)
+    solver = SolverWCSPH(model, cfg)
+    fa, fc = model.state(), model.state()
+    fwd_graph = FrameGraph(solver, fa, fc, dt, substeps=steps, warmup=False)
+
+    def forward_only():  # the plain substeps, all of them in one CUDA graph
+        fa.particle_q.copy_(x0)
+        fa.particle_qd.zero_()
+        fwd_graph.replay()
+
+    def forward_eager():
+        a, c = model.state(), model.state()
+        for _ in range(steps):
+            solver.step(a, c, None, None, dt)
+            a, c = c, a
+
+    def fwd_bwd(which=sim):
+        leaves = [x0.clone().requires_grad_(), torch.zeros_like(x0).requires_grad_()] + \
+                 [t.clone().requires_grad_() for t in (stiff, visc, rest)]
+        xT, _ = which.rollout(*leaves, steps)
+        loss = ((xT - target) ** 2).sum(1).mean()
+        loss.backward()
+        return leaves
+
+    def timed(fn):
+        fn()  # warm-up (records the CUDA graphs)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = fn()
+            e1.record()
+            flush.zero_()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts), out
+
+    t_f, _ = timed(forward_only)
+    t_fe, _ = timed(forward_eager)
+    t_fb, leaves = timed(fwd_bwd)
+    t_fbr, _ = timed(lambda: fwd_bwd(sim_replay))
+    gnorm = {nm: float(t.grad.norm()) for nm, t in zip(("x0", "v0", "stiffness", "viscosity", "rest_density"),
+                                                        leaves)}
+    rec = dict(desc, solver="WCSPH", dt=dt, substeps=steps, checkpoint_every=k, value=round(n * steps / (t_fb * 1e-3), 1),
+               unit="particle-steps/s (forward + backward)", ms_forward=round(t_f, 3),
+               ms_forward_eager=round(t_fe, 3), ms_forward_backward=round(t_fb, 3),
+               ratio_fwd_bwd_to_forward=round(t_fb / t_f, 3), ratio_fwd_bwd_to_forward_eager=round(t_fb / t_fe, 3),
+               segment_records_kept=min(sim.max_records, (steps + k - 1) // k),
+               replay_all_but_last=dict(ms_forward_backward=round(t_fbr, 3), ratio_fwd_bwd_to_forward=round(t_fbr / t_f, 3),
+                                        record_bytes=0),
+               forward_value=round(n * steps / (t_f * 1e-3), 1), grad_norms=gnorm,
+               forward="plain WCSPH substeps replayed from one CUDA graph (eager: one solver.step per substep)",
+               backward="DiffWCSPH: checkpoints every k substeps; segment records kept within a quarter of free "
+                        "device memory, other segments replayed; CUDA graph per segment")
+    del sim, sim_replay, solver, model, fwd_graph
+    torch.cuda.empty_cache()
+    return rec
+
+
 # --------------------------------------------------------------- clocks ----
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -445,6 +544,9 @@ def run_ours(args):
     if world == 1 and not args.no_secondary and not args.no_batched:
         for kind in ("pbf", "wcsph"):
             secondary[f"batched_{kind}_256"] = time_batched(kind, dev, flush)
+    if world == 1 and not args.no_secondary and not args.no_adjoint:
+        secondary["adjoint_wcsph_50232"] = time_adjoint(dev, flush)
+        secondary["batched_adjoint_wcsph_256"] = time_adjoint(dev, flush, batched=True)
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline and not args.workload.startswith("wcsph_stress"):
@@ -519,6 +621,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -13,7 +13,8 @@
 //   pres_ij = -m_j (P_i + P_j),                   grad W(d) = gs(r) d
 //   u' = v + dt a;  x' = x + dt u';  walls(x', u')
 // Given the adjoints of the outputs (xb', vb') the three passes compute:
-//   integrate  elementwise: walls^T and the integrator -> ab_i (+ own xb, vb)
+//   prepare    elementwise: cell-order copies of the step's data, and
+//              walls^T and the integrator -> ab_i
 //   force      per particle k, both sides of every pair (k, j): its own term
 //              of a_k (weights ab_k) and its term in a_j (weights ab_j), so
 //              each thread sums into its own slot (a gather, no atomics):
@@ -26,10 +27,6 @@
 #include "fs_nbr.cuh"
 
 namespace fs {
-
-__global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x,
-                                const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
-                                float* __restrict__ mv, uint32_t* status, int nworlds);
 
 namespace {
 
@@ -79,6 +76,8 @@ struct AdjArgs {
   const float* coh;    // surface_tension / mass, cell order
   float4* ab;          // (ab, 0), cell order
   float4* xr;          // (xb partial, rhob), cell order
+  const float* xin;    // step input positions, original order
+  const float* vin;    // step input velocities
   const float* accel;  // forward accel, original order
   const float* rho;    // forward rho, original order
   const float* pressure;
@@ -94,26 +93,33 @@ struct AdjArgs {
   Walls walls;
 };
 
-// gathers of the per-particle coefficients of the force adjoint
-__global__ void k_adj_gather(int64_t n, const int32_t* __restrict__ perm, fs_model m, float* __restrict__ nu,
-                             float* __restrict__ coh) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const int32_t i = perm[s];
-  nu[s] = m.viscosity[i];
-  coh[s] = m.surface_tension[i] / m.particle_mass[i];
-}
-
-__global__ void k_adj_integrate(AdjArgs a) {
+// Cell-order copies of what the adjoint passes read (one kernel): positions
+// + flags, velocities + mass, mv, (P, R) from the step's rho and pressure,
+// viscosity, cohesion / mass, and ab from the walls / integrator adjoint.
+__global__ void k_adj_prepare(AdjArgs a, float* __restrict__ nu, float* __restrict__ coh, float4* __restrict__ xs,
+                              float4* __restrict__ vs, float* __restrict__ mv, float2* __restrict__ sc2) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
-  const float4 xi = a.xs[s];
+  const int32_t i = a.g.perm[s];
+  const fs_model& m = a.m;
+  const float3 x = ld3(a.xin, i), v = ld3(a.vin, i);
+  const int pf = particle_pf(m.particle_flags, m.particle_mask, i);
+  const int w = (a.g.nworlds > 0 && m.particle_world) ? world_index(m.particle_world[i], a.g.nworlds) : 0;
+  const float4 x4 = make_float4(x.x, x.y, x.z, pack_pf(pf, w));
+  const float mass = m.particle_mass[i];
+  xs[s] = x4;
+  vs[s] = make_float4(v.x, v.y, v.z, mass);
+  const float rd = m.rest_density[i];
+  mv[s] = rd * (mass / fmaxf(rd, 1.0e-6f));
+  const float r = a.rho[i];
+  sc2[s] = make_float2(a.pressure[i] / fmaxf(r * r, 1.0e-6f), 1.0f / fmaxf(r, 1.0e-6f));
+  nu[s] = m.viscosity[i];
+  coh[s] = m.surface_tension[i] / mass;
   float3 ab = make_float3(0.f, 0.f, 0.f);
-  if (pf_of(xi) & PF_DYNAMIC) {
-    const int32_t i = a.g.perm[s];
+  if (pf & PF_DYNAMIC) {
     float3 xb, vb;
-    integrate_adjoint(walls_of(a.walls, a.g, world_of(xi)), xyz(xi), xyz(a.vs[s]), ld3(a.accel, i), a.dt,
-                      ld3(a.xbo, i), ld3(a.vbo, i), xb, vb, ab);
+    integrate_adjoint(walls_of(a.walls, a.g, w), x, v, ld3(a.accel, i), a.dt, ld3(a.xbo, i), ld3(a.vbo, i), xb, vb,
+                      ab);
   }
   a.ab[s] = make_float4(ab.x, ab.y, ab.z, 0.f);
 }
@@ -273,14 +279,6 @@ __global__ void __launch_bounds__(kNbBlock) k_adj_density(AdjArgs a) {
   st3(a.xbi, i, xb);
 }
 
-__global__ void k_gather_ratios_adj(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ rho,
-                                    const float* __restrict__ p, float2* __restrict__ out) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const int32_t i = perm[s];
-  const float r = rho[i];
-  out[s] = make_float2(p[i] / fmaxf(r * r, 1.0e-6f), 1.0f / fmaxf(r, 1.0e-6f));
-}
 
 }  // namespace
 }  // namespace fs
@@ -308,13 +306,6 @@ int fs_wcsph_substep_adjoint(fs_context* c, const fs_model* m, const fs_state* s
   const float h = p->smoothing_length;
   int rc;
   if ((rc = grid_build(c, si->particle_q, n, h, st, m->particle_world))) return rc;
-  {
-    PassScope ps_(c, P_GATHER, st, 3);
-    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, si->particle_q, si->particle_qd, c->xs, c->vs,
-                                                    c->mv, c->status, c->nworlds);
-    k_gather_ratios_adj<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, rho, pressure, c->sc2);
-    k_adj_gather<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, c->sc1, c->sc1b);
-  }
   AdjArgs a;
   a.g = grid_view(c);
   a.L = nbr_list(c);
@@ -328,6 +319,8 @@ int fs_wcsph_substep_adjoint(fs_context* c, const fs_model* m, const fs_state* s
   a.coh = c->sc1b;
   a.ab = c->xs2;
   a.xr = c->vs2;
+  a.xin = si->particle_q;
+  a.vin = si->particle_qd;
   a.accel = accel;
   a.rho = rho;
   a.pressure = pressure;
@@ -345,7 +338,7 @@ int fs_wcsph_substep_adjoint(fs_context* c, const fs_model* m, const fs_state* s
   a.walls = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 0, 0.f, 0.f);
   {
     PassScope ps_(c, P_ADJ_INTEGRATE, st);
-    k_adj_integrate<<<blocks_for(n), kBlock, 0, st>>>(a);
+    k_adj_prepare<<<blocks_for(n), kBlock, 0, st>>>(a, c->sc1, c->sc1b, c->xs, c->vs, c->mv, c->sc2);
   }
   {
     PassScope ps_(c, P_ADJ_FORCE, st);

@@ -15,14 +15,18 @@ GRAVITY = (0.0, 0.0, -10.0)
 DT = 1.0e-4
 
 
-def block(side=11, squeeze=0.94, seed=0, sigma=0.3):
-    """side^3 particles squeezed to 94 % of the spacing, resting on the floor
-    and touching the -x wall; velocities N(0, sigma)."""
+def block(side=11, squeeze=0.94, seed=0, sigma=0.3, at_wall=True):
+    """side^3 particles squeezed to 94 % of the spacing, velocities
+    N(0, sigma); resting on the floor against the -x wall (at_wall) or
+    floating in the middle of the tank, clear of every wall."""
     rng = np.random.default_rng(seed)
     g = np.arange(side) * SPACING * squeeze
     x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
     x = x + rng.uniform(-0.03, 0.03, x.shape) * SPACING
-    x = x + np.array([-CFG["bound_width"] + 0.1 * SPACING, -0.5 * g[-1], 0.1 * SPACING])
+    if at_wall:
+        x = x + np.array([-CFG["bound_width"] + 0.1 * SPACING, -0.5 * g[-1], 0.1 * SPACING])
+    else:
+        x = x + np.array([-0.5 * g[-1], -0.5 * g[-1], CFG["bound_length"] - 0.5 * g[-1]])
     v = rng.normal(size=x.shape) * sigma
     return x.astype(np.float32), v.astype(np.float32)
 

@@ -5,11 +5,16 @@ behind fluid_simulation_b200.diff.DiffWCSPH).
     forward is pinned to the FP64 oracle in test_wcsph_tape.py) after one
     and after 20 substeps of a compressed block against the walls, with
     pressure, viscosity, cohesion and walls active: 1e-3 norm-relative;
-  - checkpointing every 1, 7 or 10 substeps gives bit-identical gradients;
-  - against FP64 central finite differences of the CPU oracle on a dam-break
-    column, loss = mean squared distance to the column moved by +0.3 m in x,
-    along random directions of v0 and along stiffness and rest density
-    (eps = 1e-4 relative): 1e-3 relative.
+  - checkpointing every 1, 7 or 10 substeps, with segment records kept or
+    segments replayed, gives bit-identical gradients;
+  - against FP64 central finite differences of the CPU oracle, loss = mean
+    squared distance to the initial cloud moved by +0.3 m in x, along random
+    directions of v0 (a dam-break column) and of v0, stiffness, viscosity
+    and rest density (a compressed block clear of the walls), eps = 1e-4
+    relative: 1e-3 relative.  Finite differences are taken away from walls:
+    a wall clamps positions and damps velocities discontinuously, so a
+    difference quotient across a wall contact is no derivative (the tape
+    tests above cover the walls' adjoint).
 """
 
 import numpy as np
@@ -28,11 +33,11 @@ pytestmark = pytest.mark.gpu
 GTOL = 1e-3
 
 
-def diff_sim(x, prm, dev, k=10, cfg=CFG, dt=DT, mass=MASS):
+def diff_sim(x, prm, dev, k=10, cfg=CFG, dt=DT, mass=MASS, record_bytes=None):
     m = model_from_arrays(x, np.zeros_like(x), mass, device=dev, radius=cfg["particle_radius"],
                           gravity=(GRAVITY,), attributes=dict(prm, particle_mask=0), solver_cls=SolverWCSPH)
     c = SolverWCSPH.SphConfig(**cfg)
-    return DiffWCSPH(m, c, dt, checkpoint_every=k)
+    return DiffWCSPH(m, c, dt, checkpoint_every=k, record_bytes=record_bytes)
 
 
 def gpu_grads(sim, x, v, prm, steps, loss_fn, dev):
@@ -81,17 +86,37 @@ def test_adjoint_matches_tape(steps, cuda_device):
 
 
 def test_gradients_do_not_depend_on_checkpoint_interval(cuda_device):
+    """Checkpoint intervals 1, 7, 10, each with every segment's record kept
+    and with all but the last segment replayed: identical bits."""
     x, v = block(side=9, seed=3)
     prm = params(len(x), seed=4)
     loss = weighted_loss(len(x), 6)
     ref = None
     for k in (1, 7, 10):
-        g = gpu_grads(diff_sim(x, prm, cuda_device, k=k), x, v, prm, 25, loss, cuda_device)
-        if ref is None:
-            ref = g
-        else:
-            for nm, a, b in zip(NAMES, g, ref):
-                assert np.array_equal(a, b), (k, nm)
+        for record_bytes in (None, 0):
+            sim = diff_sim(x, prm, cuda_device, k=k, record_bytes=record_bytes)
+            assert (sim.max_records >= 25) == (record_bytes is None)
+            g = gpu_grads(sim, x, v, prm, 25, loss, cuda_device)
+            if ref is None:
+                ref = g
+            else:
+                for nm, a, b in zip(NAMES, g, ref):
+                    assert np.array_equal(a, b), (k, record_bytes, nm)
+
+
+def test_graph_replayed_rollouts_equal_eager_ones(cuda_device):
+    x, v = block(side=9, seed=7)
+    prm = params(len(x), seed=8)
+    loss = weighted_loss(len(x), 9)
+    out = []
+    for graphs in (False, True):
+        sim = diff_sim(x, prm, cuda_device, k=5)
+        sim.use_graphs = graphs
+        for _ in range(3):  # eager first run, recording, then replays
+            g = gpu_grads(sim, x, v, prm, 15, loss, cuda_device)
+        out.append(g)
+    for nm, a, b in zip(NAMES, out[0], out[1]):
+        assert np.array_equal(a, b), nm
 
 
 def test_rollout_forward_equals_plain_substeps(cuda_device):
@@ -142,7 +167,7 @@ def oracle_loss(x0, v0, prm, cfg, dt, steps, mass, target):
 def test_gradients_match_fp64_finite_differences(case, cuda_device):
     """dam: a make_scene(5000) column at rest, 40 substeps at the acoustic dt
     (its pressure stays clamped at zero this early, so only v0 is checked);
-    block: the compressed block against the walls, 20 substeps, where
+    block: the compressed block clear of the walls, 20 substeps, where
     stiffness, viscosity and rest density all act."""
     if case == "dam":
         s, cfg, prm, dt, steps = dam_case()
@@ -150,7 +175,7 @@ def test_gradients_match_fp64_finite_differences(case, cuda_device):
         v0 = np.zeros_like(x0)
         fields = ()
     else:
-        x0, v0 = block()
+        x0, v0 = block(at_wall=False)
         prm, cfg, dt, steps, mass = params(len(x0)), CFG, DT, 20, MASS
         fields = (("stiffness", 2), ("viscosity", 3), ("rest_density", 4))
     n = len(x0)
