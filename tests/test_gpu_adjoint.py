@@ -17,6 +17,8 @@ behind fluid_simulation_b200.diff.DiffWCSPH).
     tests above cover the walls' adjoint).
 """
 
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -205,3 +207,49 @@ def test_gradients_match_fp64_finite_differences(case, cuda_device):
     for name, ad, fd in checks:
         assert fd != 0.0, name
         assert abs(ad - fd) <= GTOL * abs(fd), (name, ad, fd)
+
+
+def test_dam_break_50k_gradients_match_finite_differences(cuda_device):
+    """The differentiable dam-break workload at full size: make_scene(50000)
+    (50,232 particles), 120 substeps at the acoustic dt, checkpoints every 10
+    substeps with every segment but the last replayed; FP64 central finite
+    differences of the oracle along 32 random unit directions of v0 (eps =
+    1e-4 m/s).  In these 26 ms the column falls freely (it starts 3 cm above
+    the floor and below rest density, so the clamped pressure stays zero and
+    all velocities stay equal): the stiffness, viscosity and rest-density
+    gradients are exactly zero, as the finite differences confirm.
+    The oracle needs about 2 s per FP64 rollout on 16 host threads, so the
+    default run checks 4 directions; FS_FD_DIRECTIONS=32 runs all 32."""
+    ndir = int(os.environ.get("FS_FD_DIRECTIONS", "4"))
+    s, cfg, prm, dt, _ = dam_case(50000)
+    steps = 120
+    x0 = s.positions
+    n = len(x0)
+    v0 = np.zeros_like(x0)
+    target = x0.astype(np.float64) + np.array([0.3, 0.0, 0.0])
+    tgt = torch.tensor(target, dtype=torch.float32, device=cuda_device)
+
+    def loss(xT, vT):
+        return ((xT - tgt) ** 2).sum(1).mean()
+
+    sim = diff_sim(x0, prm, cuda_device, k=10, cfg=cfg, dt=dt, mass=s.mass, record_bytes=0)
+    g = gpu_grads(sim, x0, v0, prm, steps, loss, cuda_device)
+    rng = np.random.default_rng(2)
+    eps = 1e-4
+    worst = 0.0
+    for _ in range(ndir):
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d)
+        fd = (oracle_loss(x0, v0 + eps * d, prm, cfg, dt, steps, s.mass, target) -
+              oracle_loss(x0, v0 - eps * d, prm, cfg, dt, steps, s.mass, target)) / (2 * eps)
+        ad = float(np.sum(g[1] * d))
+        worst = max(worst, abs(ad - fd) / abs(fd))
+    print(f"worst relative error over {ndir} directions", worst)
+    assert worst <= GTOL
+    for key, gi in (("stiffness", 2), ("viscosity", 3), ("rest_density", 4)):
+        hi = dict(prm, **{key: prm[key].astype(np.float64) * (1 + eps)})
+        lo = dict(prm, **{key: prm[key].astype(np.float64) * (1 - eps)})
+        fd = (oracle_loss(x0, v0, hi, cfg, dt, steps, s.mass, target) -
+              oracle_loss(x0, v0, lo, cfg, dt, steps, s.mass, target)) / (2 * eps)
+        assert float(np.abs(g[gi]).max()) == 0.0, key
+        assert abs(fd) <= 1e-9, (key, fd)
