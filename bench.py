@@ -61,6 +61,42 @@ FALLBACK_HBM_GBS = 6650.0
 SUBSTEP_DT = {"pbf": 1.0 / 240.0, "dfsph": 1.0 / 240.0}
 
 
+class HarnessClock:
+    """The reference harness's substep sizes (simulation.py:155-190): PBF
+    takes frame_dt / 4; DFSPH takes min(rest of the frame, frame_dt / 4,
+    0.4 spacing / max|v|) before every substep.  The speed is a device
+    max-norm reduction (fs_norm_maxima) read back between timed steps, never
+    inside one; ``speed_of`` replaces it for numpy states (CPU runs)."""
+
+    def __init__(self, kind, spacing, frame_dt=1.0 / 60.0, substeps=4):
+        self.kind, self.spacing = kind, float(spacing)
+        self.frame_dt, self.limit = frame_dt, frame_dt / substeps
+        self.remaining = frame_dt
+        self._out = None
+
+    def _speed(self, v):
+        if isinstance(v, np.ndarray):
+            return float(np.sqrt((v.astype(np.float64) ** 2).sum(1).max())) if len(v) else 0.0
+        import torch
+        from fluid_simulation_b200 import _lib
+        if self._out is None:
+            self._out = torch.zeros(2, dtype=torch.float32, device=v.device)
+        _lib.check(_lib.load().fs_norm_maxima(v.data_ptr(), v.shape[0], None, 0, self._out.data_ptr(),
+                                              torch.cuda.current_stream(v.device).cuda_stream), "norm maxima")
+        return float(self._out[0].item()) ** 0.5
+
+    def next(self, v):
+        if self.kind != "dfsph":
+            return self.limit
+        speed = self._speed(v)
+        dt = self.limit if speed <= 0.0 else min(self.limit, 0.4 * self.spacing / speed)
+        dt = min(self.remaining, dt)
+        self.remaining -= dt
+        if self.remaining <= 1.0e-12:
+            self.remaining = self.frame_dt
+        return dt
+
+
 def measured_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -85,7 +121,8 @@ def build_workload(name, device):
                               gravity=(s.spec.gravity,), attributes=attrs, solver_cls=cls)
         solver = cls(m, solver_config(kind, s))
         desc = dict(workload=name, particles=s.count, scene="make_scene(400000) dam break",
-                    solver=kind.upper(), dt=SUBSTEP_DT[kind])
+                    solver=kind.upper(), dt=SUBSTEP_DT[kind] if kind == "pbf" else
+                    "harness CFL: min(rest of frame, 1/240, 0.4 spacing / max|v|)", spacing=s.spacing)
         if kind == "pbf":
             desc.update(constraint_iterations=4, substeps_per_frame=4, artificial_pressure="off (harness scorr_k=0)",
                         xsph_c=0.05)
@@ -136,12 +173,12 @@ def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1):
     import oracle
     kind, model, state, cfg, n = cpu_oracle_setup(name)
     step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step}[kind]
-    dt = SUBSTEP_DT[kind]
+    clock = HarnessClock(kind, cfg["particle_length"])
     cores = oracle.num_threads(os.cpu_count() or 1)
     k = 0
     t0 = time.perf_counter()
     while k < max_steps and (k < min_steps or time.perf_counter() - t0 < max_seconds):
-        out = step(model, state, cfg, dt)[0]
+        out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
         state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
         k += 1
     el = time.perf_counter() - t0
@@ -431,13 +468,17 @@ def run_ours(args):
     a, b = model.state(), model.state()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    def step():
+    clock = HarnessClock(desc["solver"].lower(), desc.get("spacing", 0.0))
+    if desc["solver"] == "WCSPH":
+        clock.next = lambda v: dt  # the stress lattice runs at its fixed acoustic dt
+
+    def step(dt_k):
         nonlocal a, b
-        solver.step(a, b, None, None, dt)
+        solver.step(a, b, None, None, dt_k)
         a, b = b, a
 
     for _ in range(args.warmup):
-        step()
+        step(clock.next(a.particle_qd))
     torch.cuda.synchronize()
 
     K = args.steps
@@ -452,8 +493,9 @@ def run_ours(args):
     time.sleep(0.3)
     launches0 = lib.fs_launch_count(ctx)
     for k in range(K):
+        dt_k = clock.next(a.particle_qd)  # DFSPH: reads back max|v| (outside the events)
         ev[k][0].record()
-        step()
+        step(dt_k)
         ev[k][1].record()
         flush.zero_()
     torch.cuda.synchronize()
@@ -495,10 +537,15 @@ def run_ours(args):
     ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(Ke)]
     s_in, s_out = model.state(), model.state()
     for k in range(Ke):
+        if clock.kind == "dfsph":  # the harness reads max|v| back before each substep
+            torch.cuda.current_stream(dev).synchronize()
+            dt_k = clock.next(hv.numpy())
+        else:
+            dt_k = clock.next(None)
         ee[k][0].record()
         s_in.particle_q.copy_(hx, non_blocking=True)
         s_in.particle_qd.copy_(hv, non_blocking=True)
-        solver.step(s_in, s_out, None, None, dt)
+        solver.step(s_in, s_out, None, None, dt_k)
         hx.copy_(s_out.particle_q, non_blocking=True)
         hv.copy_(s_out.particle_qd, non_blocking=True)
         ee[k][1].record()
@@ -517,17 +564,21 @@ def run_ours(args):
             if wl == args.workload:
                 continue
             m2, s2, dt2, n2, d2 = build_workload(wl, dev)
+            c2 = HarnessClock(d2["solver"].lower(), d2.get("spacing", 0.0))
+            if d2["solver"] == "WCSPH":
+                c2.next = lambda v: dt2
             x0, x1 = m2.state(), m2.state()
             for _ in range(3):
-                s2.step(x0, x1, None, None, dt2)
+                s2.step(x0, x1, None, None, c2.next(x0.particle_qd))
                 x0, x1 = x1, x0
             torch.cuda.synchronize()
             k2 = max(5, min(30, K))
             tot = 0.0
             for _ in range(k2):
+                dt_k = c2.next(x0.particle_qd)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()
-                s2.step(x0, x1, None, None, dt2)
+                s2.step(x0, x1, None, None, dt_k)
                 e1.record()
                 x0, x1 = x1, x0
                 flush.zero_()
@@ -583,14 +634,14 @@ def run_reference(args):
     import oracle
     cores = oracle.num_threads(os.cpu_count() or 1)
     step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step}[kind]
-    dt = SUBSTEP_DT[kind]
+    clock = HarnessClock(kind, cfg["particle_length"])
     for _ in range(min(args.warmup, 1)):
-        out = step(model, state, cfg, dt)[0]
+        out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
         state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
     k = 0
     t0 = time.perf_counter()
     while k < args.steps and (k == 0 or time.perf_counter() - t0 < args.cpu_seconds * 3):
-        out = step(model, state, cfg, dt)[0]
+        out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
         state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
         k += 1
     el = time.perf_counter() - t0
@@ -602,7 +653,8 @@ def run_reference(args):
         impl="reference", metric="particle-steps/s", value=round(value, 1), unit="particle-steps/s", n_gpus=0,
         steps=k, warmup=min(args.warmup, 1), ms_per_step=round(el / k * 1e3, 3), higher_is_better=True,
         scaling="weak", vs_baseline=None, dtype="f32", data="synthetic (reference dam-break scene generator)",
-        config=dict(workload=args.workload, particles=n, dt=dt),
+        config=dict(workload=args.workload, particles=n, dt=SUBSTEP_DT[kind] if kind == "pbf" else
+                    "harness CFL: min(rest of frame, 1/240, 0.4 spacing / max|v|)"),
         cpu_baseline=dict(value=round(value, 1), unit="particle-steps/s", cores=cores, kind="port", sample=sample),
         e2e=dict(value=round(value, 1), unit="particle-steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
     )), flush=True)

@@ -177,7 +177,7 @@ FS_DEV PairAdj pair_adjoint(const Cubic& K, float h, float particle_radius, floa
   return o;
 }
 
-__global__ void __launch_bounds__(kNbBlock) k_adj_force(AdjArgs a) {
+__global__ void FS_NB_BOUNDS k_adj_force(AdjArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   lists_recorded(a.L);
   if (s >= a.n) return;
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kNbBlock) k_adj_force(AdjArgs a) {
   st3(a.vbi, i, vb);
 }
 
-__global__ void __launch_bounds__(kNbBlock) k_adj_density(AdjArgs a) {
+__global__ void FS_NB_BOUNDS k_adj_density(AdjArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xk = a.xs[s];

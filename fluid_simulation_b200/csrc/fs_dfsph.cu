@@ -63,7 +63,7 @@ struct DensFactorArgs {
 
 // Records the neighbour lists of this grid (positions stay fixed for the half
 // step, so every later pass of the half reuses them exactly).
-__global__ void __launch_bounds__(kNbBlock) k_density_factor(DensFactorArgs a) {
+__global__ void FS_NB_BOUNDS k_density_factor(DensFactorArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   lists_recorded(a.L);
   if (s >= a.n) return;
@@ -117,7 +117,7 @@ struct AccelArgs {
   float4* vstar;     // cell order (v*, mass)
 };
 
-__global__ void __launch_bounds__(kNbBlock) k_accel_predict(AccelArgs a) {
+__global__ void FS_NB_BOUNDS k_accel_predict(AccelArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
@@ -252,7 +252,7 @@ __device__ bool last_block(uint32_t* ticket) {
   return am_last;
 }
 
-__global__ void __launch_bounds__(kNbBlock) k_rate(RateArgs a) {
+__global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
   if (a.ctrl && a.ctrl->done) return;  // uniform across the grid: set by an earlier launch
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double term = 0.0;
@@ -320,7 +320,7 @@ struct CorrectArgs {
   const DfsphDev* ctrl;
 };
 
-__global__ void __launch_bounds__(kNbBlock) k_correct(CorrectArgs a) {
+__global__ void FS_NB_BOUNDS k_correct(CorrectArgs a) {
   if (a.ctrl && a.ctrl->done) return;
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;

@@ -308,9 +308,9 @@ FS_DEV int world_cell_key(const WorldDev& W, float inv, float px, float py, floa
 }
 
 // The query cells of world w in the order z-outer, y, x-inner; each row of
-// x cells is one contiguous slot range.
-template <class F>
-FS_DEV void for_each_candidate_world(const GridDev& g, int w, float px, float py, float pz, float r, F&& f) {
+// x cells is one contiguous slot range, passed to rf(first, end).
+template <class RF>
+FS_DEV void for_each_range_world(const GridDev& g, int w, float px, float py, float pz, float r, RF&& rf) {
   const WorldDev& W = g.worlds[world_index(w, g.nworlds)];
   auto cell = [&](float v, int k) { return world_axis_cell(v, g.inv, W.clo[k], W.dims[k]); };
   const int x0 = cell(__fsub_rn(px, r), 0), x1 = cell(__fadd_rn(px, r), 0);
@@ -319,26 +319,17 @@ FS_DEV void for_each_candidate_world(const GridDev& g, int w, float px, float py
   for (int z = z0; z <= z1; ++z)
     for (int y = y0; y <= y1; ++y) {
       const int row = W.base + (z * W.dims[1] + y) * W.dims[0];
-      const int e = __ldg(g.off + row + x1 + 1);
-      for (int t = __ldg(g.off + row + x0); t < e; ++t) f(t);
+      rf(__ldg(g.off + row + x0), __ldg(g.off + row + x1 + 1));
     }
 }
 
-template <class F>
-FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f);
-
-// The candidates of a query at (px, py, pz) of world w (w is ignored by the
-// reference hash grid).
-template <class F>
-FS_DEV void for_each_candidate(const GridDev& g, int w, float px, float py, float pz, float r, F&& f) {
-  if (g.worlds)
-    for_each_candidate_world(g, w, px, py, pz, r, f);
-  else
-    for_each_candidate(g, px, py, pz, r, f);
-}
-
-template <class F>
-FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f) {
+// Visits the candidates of warp's hash_grid_query(grid, p, r) in the same
+// order as contiguous slot ranges rf(first, end): cells z-outer, y-middle,
+// x-inner, each cell's slots in sorted order.  A run of consecutive x cells
+// is one range because cell offsets are a prefix sum in hash-key order; a
+// run that wraps modulo dim_x splits in two.
+template <class RF>
+FS_DEV void for_each_range_hash(const GridDev& g, float px, float py, float pz, float r, RF&& rf) {
   const int x0 = to_cell(__fmul_rn(__fsub_rn(px, r), g.inv), g.rounding);
   const int y0 = to_cell(__fmul_rn(__fsub_rn(py, r), g.inv), g.rounding);
   const int z0 = to_cell(__fmul_rn(__fsub_rn(pz, r), g.inv), g.rounding);
@@ -354,23 +345,42 @@ FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, f
       if (xa >= 0) {
         const int cx0 = g.mask_x >= 0 ? (xa & g.mask_x) : xa % g.dim_x;
         const int len1 = min(nx, g.dim_x - cx0);
-        int s = __ldg(g.off + row + cx0);
-        int e = __ldg(g.off + row + cx0 + len1);
-        for (int t = s; t < e; ++t) f(t);
-        if (nx > len1) {
-          s = __ldg(g.off + row);
-          e = __ldg(g.off + row + (nx - len1));
-          for (int t = s; t < e; ++t) f(t);
-        }
+        rf(__ldg(g.off + row + cx0), __ldg(g.off + row + cx0 + len1));
+        if (nx > len1) rf(__ldg(g.off + row), __ldg(g.off + row + (nx - len1)));
       } else {  // far outside the shifted range: cells clamp, visit one by one
         for (int x = x0; x <= x1; ++x) {
           const int c = row + wrap_axis(x, g.dim_x, g.mask_x);
-          const int e = __ldg(g.off + c + 1);
-          for (int t = __ldg(g.off + c); t < e; ++t) f(t);
+          rf(__ldg(g.off + c), __ldg(g.off + c + 1));
         }
       }
     }
   }
+}
+
+// The candidate ranges of a query at (px, py, pz) of world w (w is ignored
+// by the reference hash grid).
+template <class RF>
+FS_DEV void for_each_range(const GridDev& g, int w, float px, float py, float pz, float r, RF&& rf) {
+  if (g.worlds)
+    for_each_range_world(g, w, px, py, pz, r, rf);
+  else
+    for_each_range_hash(g, px, py, pz, r, rf);
+}
+
+// The same candidates one slot at a time: f(t), t = cell-sorted SLOT
+// (original index = perm[t]).
+template <class F>
+FS_DEV void for_each_candidate(const GridDev& g, int w, float px, float py, float pz, float r, F&& f) {
+  for_each_range(g, w, px, py, pz, r, [&](int a, int e) {
+    for (int t = a; t < e; ++t) f(t);
+  });
+}
+
+template <class F>
+FS_DEV void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f) {
+  for_each_range_hash(g, px, py, pz, r, [&](int a, int e) {
+    for (int t = a; t < e; ++t) f(t);
+  });
 }
 
 // Box walls of the reference's apply_bounds variants.

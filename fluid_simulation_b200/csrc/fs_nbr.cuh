@@ -15,6 +15,18 @@ namespace fs {
 
 constexpr int kNbBlock = 128;  // threads per block of neighbour kernels
 
+// Launch bounds of the neighbour kernels: the minimum number of resident
+// blocks per SM sets the register budget the compiler may use
+// (65536 / (kNbBlock * min blocks)); 0 leaves it to the compiler.
+#ifndef FS_NB_MIN_BLOCKS
+#define FS_NB_MIN_BLOCKS 0
+#endif
+#if FS_NB_MIN_BLOCKS > 0
+#define FS_NB_BOUNDS __launch_bounds__(kNbBlock, FS_NB_MIN_BLOCKS)
+#else
+#define FS_NB_BOUNDS __launch_bounds__(kNbBlock)
+#endif
+
 // support test margin: FMA-evaluated r^2 may differ from the individually
 // rounded r^2 by about one ulp; anything the reference counts (r <= h) passes
 constexpr float kSupportMargin = 1.000002f;
@@ -113,15 +125,30 @@ template <bool COUNT>
 FS_DEV int record_list(const GridDev& g, const float4* __restrict__ xs, int s, float4 xi, float h, float h2m,
                        const NbrList& L) {
   int n = 0, ncand = 0;
-  for_each_candidate(g, world_of(xi), xi.x, xi.y, xi.z, h, [&](int t) {
-    const float4 xj = __ldg(xs + t);
+  int32_t* out = L.idx + s;  // entry n of slot s lives at out[n * stride]
+  const int64_t stride = L.stride;
+  auto test = [&](int t, float4 xj) {
     if (COUNT) ncand += (t != s) ? (__float_as_int(xj.w) & PF_ACTIVE) : 0;
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xj.w)));  // +inf for inactive
     if (r2 <= h2m) {
-      if (n < kNbMax) L.idx[(int64_t)n * L.stride + s] = t;
+      if (n < kNbMax) {
+        *out = t;
+        out += stride;
+      }
       ++n;
     }
+  };
+  for_each_range(g, world_of(xi), xi.x, xi.y, xi.z, h, [&](int a, int e) {
+    int t = a;
+    for (; t + 4 <= e; t += 4) {  // four independent loads in flight
+      const float4 x0 = __ldg(xs + t), x1 = __ldg(xs + t + 1), x2 = __ldg(xs + t + 2), x3 = __ldg(xs + t + 3);
+      test(t, x0);
+      test(t + 1, x1);
+      test(t + 2, x2);
+      test(t + 3, x3);
+    }
+    for (; t < e; ++t) test(t, __ldg(xs + t));
   });
   L.cnt[s] = n <= kNbMax ? n : kNbMax + 1;
   return ncand;
@@ -165,13 +192,15 @@ FS_DEV void visit(const GridDev& g, const float4* __restrict__ xs, int s, float4
       if (fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xj.w))) <= h2m && (WITH_SELF || t != s)) pair(t, xj);
     };
     int k = 0;
-    for (; k + 1 < n; k += 2) {  // two independent gathers in flight
-      const int t0 = entry(k), t1 = entry(k + 1);
-      const float4 x0 = __ldg(xs + t0), x1 = __ldg(xs + t1);
+    for (; k + 3 < n; k += 4) {  // four independent gathers in flight
+      const int t0 = entry(k), t1 = entry(k + 1), t2 = entry(k + 2), t3 = entry(k + 3);
+      const float4 x0 = __ldg(xs + t0), x1 = __ldg(xs + t1), x2 = __ldg(xs + t2), x3 = __ldg(xs + t3);
       one(t0, x0);
       one(t1, x1);
+      one(t2, x2);
+      one(t3, x3);
     }
-    if (k < n) {
+    for (; k < n; ++k) {
       const int t0 = entry(k);
       one(t0, __ldg(xs + t0));
     }

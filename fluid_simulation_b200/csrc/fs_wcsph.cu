@@ -62,7 +62,7 @@ struct DensityArgs {
   float2* sc2;                // cell order
 };
 
-__global__ void __launch_bounds__(kNbBlock) k_wcsph_density(DensityArgs a) {
+__global__ void FS_NB_BOUNDS k_wcsph_density(DensityArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   lists_recorded(a.L);
   if (s >= a.n) return;
@@ -111,7 +111,7 @@ struct ForceArgs {
   float* v_out;
 };
 
-__global__ void __launch_bounds__(kNbBlock) k_wcsph_force(ForceArgs a) {
+__global__ void FS_NB_BOUNDS k_wcsph_force(ForceArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const float4 xi = a.xs[s];
