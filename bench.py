@@ -238,6 +238,8 @@ def time_batched(kind, dev, flush, frames=2, warm=1):
     mb = batched_model(b, cls, device=dev)
     sb = cls(mb, cfg_of((1.0, 1.0, 1.0)))
     ctx_b = mb.particle_grid._ctx
+    from fluid_simulation_b200.autotune import autotune, describe
+    tuning = describe(autotune(sb, mb.state(), dt, steps=2, repeats=1))  # the serial solvers keep the default
     l0 = lib.fs_launch_count(ctx_b)
     fb = FrameGraph(sb, mb.state(), mb.state(), dt, substeps=sub, warmup=False)
     launches_b = lib.fs_launch_count(ctx_b) - l0   # kernels recorded in the frame graph
@@ -286,7 +288,7 @@ def time_batched(kind, dev, flush, frames=2, warm=1):
                serial_graph=dict(value=rate(t_serial_g), ms_per_frame=round(t_serial_g / frames, 3)),
                speedup_vs_serial_eager=round(t_serial / t_batched, 2),
                speedup_vs_serial_graph=round(t_serial_g / t_batched, 2),
-               final_state_bit_identical_to_serial=bool(same))
+               final_state_bit_identical_to_serial=bool(same), tuning_batched=tuning)
     del fb, graphs, scenes, mb, sb
     torch.cuda.empty_cache()
     return rec
@@ -471,6 +473,10 @@ def run_ours(args):
     clock = HarnessClock(desc["solver"].lower(), desc.get("spacing", 0.0))
     if desc["solver"] == "WCSPH":
         clock.next = lambda v: dt  # the stress lattice runs at its fixed acoustic dt
+    tuning = None
+    if not args.no_autotune:  # launch tuning from a few substeps of the initial state, before warm-up
+        from fluid_simulation_b200.autotune import autotune, describe
+        tuning = describe(autotune(solver, a, clock.limit if clock.kind == "dfsph" else dt))
 
     def step(dt_k):
         nonlocal a, b
@@ -568,6 +574,9 @@ def run_ours(args):
             if d2["solver"] == "WCSPH":
                 c2.next = lambda v: dt2
             x0, x1 = m2.state(), m2.state()
+            if not args.no_autotune:
+                from fluid_simulation_b200.autotune import autotune, describe
+                d2["tuning"] = describe(autotune(s2, x0, c2.limit if c2.kind == "dfsph" else dt2))
             for _ in range(3):
                 s2.step(x0, x1, None, None, c2.next(x0.particle_qd))
                 x0, x1 = x1, x0
@@ -610,6 +619,7 @@ def run_ours(args):
             vs_baseline=round(value / PUBLISHED_PBF, 3) if args.workload == "pbf_dam_401856" else None,
             dtype="f32", data="synthetic (reference dam-break scene generator, seeded)",
             config=dict(desc, l2="flushed between timed steps (512 MB write outside the events)",
+                        tuning=tuning,
                         parallelism="replicas" if world > 1 else "single GPU",
                         grid="HashGrid(128,128,128), cell = h, truncating cell coordinates"),
             e2e=dict(value=round(e2e_value, 1), unit="particle-steps/s", h2d_bytes_per_step=2 * n * 12,
@@ -674,6 +684,7 @@ def main():
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

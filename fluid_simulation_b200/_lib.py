@@ -42,6 +42,10 @@ class WorldBox(C.Structure):
                 ("bound_length", F)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("block_size", I32), ("particles_per_thread", I32), ("cell_ratio", F)]
+
+
 class Model(C.Structure):
     _fields_ = [("n", I64), ("n_worlds", I32)] + [(k, P) for k in (
         "particle_flags", "particle_mask", "particle_world", "particle_mass", "gravity", "rest_density",
@@ -88,6 +92,8 @@ SIGNATURES = {
     "fs_grid_candidates": (C.c_int, [P, P, I64, F, P, P, P, P]),
     "fs_context_create_worlds": (C.c_int, [C.POINTER(P), I64, C.POINTER(WorldBox), I32, I32]),
     "fs_context_worlds": (I32, [P]),
+    "fs_context_set_tuning": (C.c_int, [P, C.POINTER(Tuning)]),
+    "fs_context_get_tuning": (C.c_int, [P, C.POINTER(Tuning)]),
     "fs_context_cells": (I64, [P]),
     "fs_grid_build_worlds": (C.c_int, [P, P, P, I64, F, P]),
     "fs_grid_candidates_worlds": (C.c_int, [P, P, P, I64, F, P, P, P, P]),

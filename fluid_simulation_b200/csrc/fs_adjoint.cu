@@ -178,105 +178,105 @@ FS_DEV PairAdj pair_adjoint(const Cubic& K, float h, float particle_radius, floa
 }
 
 __global__ void FS_NB_BOUNDS k_adj_force(AdjArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   lists_recorded(a.L);
-  if (s >= a.n) return;
-  const float4 xk = a.xs[s];
-  const int32_t i = a.g.perm[s];
-  const int pfk = pf_of(xk);
-  if (!(pfk & PF_ACTIVE)) {  // untouched by the step: identity
-    a.L.cnt[s] = 0;
-    a.xr[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-    st3(a.xbi, i, ld3(a.xbo, i));
-    st3(a.vbi, i, ld3(a.vbo, i));
-    return;
-  }
-  const float4 vk = a.vs[s];
-  const float m_k = vk.w;
-  const float2 PRk = a.sc2[s];
-  const float nu_k = a.nu[s], coh_k = a.coh[s];
-  float3 xb = make_float3(0.f, 0.f, 0.f), vb = make_float3(0.f, 0.f, 0.f), abk = make_float3(0.f, 0.f, 0.f);
-  if (pfk & PF_DYNAMIC) {
-    integrate_adjoint(walls_of(a.walls, a.g, world_of(xk)), xyz(xk), xyz(vk), ld3(a.accel, i), a.dt, ld3(a.xbo, i),
-                      ld3(a.vbo, i), xb, vb, abk);
-  } else {
-    xb = ld3(a.xbo, i);
-    vb = ld3(a.vbo, i);
-  }
-  const Cubic K(a.h);
-  const float h2m = a.h * a.h * kSupportMargin;
-  float Pb = 0.f, Rb = 0.f, nub = 0.f;
-  record_list<false>(a.g, a.xs, (int)s, xk, a.h, h2m, a.L);
-  visit<false, true>(a.g, a.xs, (int)s, xk, a.h, h2m, a.L, true, [&](int t, float4 xj) {
-    const float3 d = make_float3(xk.x - xj.x, xk.y - xj.y, xk.z - xj.z);
-    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-    if (r2 == 0.f) return;  // the forward skips coincident pairs
-    const float4 vj = __ldg(a.vs + t);
-    const float2 PRj = __ldg(a.sc2 + t);
-    const float3 u = make_float3(vk.x - vj.x, vk.y - vj.y, vk.z - vj.z);
-    const float Psum = PRk.x + PRj.x;
-    if (pfk & PF_DYNAMIC) {  // term of a_k with neighbour j
-      const PairAdj o = pair_adjoint(K, a.h, a.particle_radius, d, r2, u, abk, nu_k, coh_k, vj.w, PRj.y, Psum);
-      xb = make_float3(xb.x + o.rb.x, xb.y + o.rb.y, xb.z + o.rb.z);
-      vb = make_float3(vb.x + o.ub.x, vb.y + o.ub.y, vb.z + o.ub.z);
-      Pb += o.pb_sum;
-      nub += o.nub;
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xk = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    const int pfk = pf_of(xk);
+    if (!(pfk & PF_ACTIVE)) {  // untouched by the step: identity
+      a.L.cnt[s] = 0;
+      a.xr[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      st3(a.xbi, i, ld3(a.xbo, i));
+      st3(a.vbi, i, ld3(a.vbo, i));
+      return;
     }
-    if (pf_of(xj) & PF_DYNAMIC) {  // term of a_j with neighbour k: d_jk = -d, u_jk = -u
-      const float4 abj4 = __ldg(a.ab + t);
-      const float3 abj = make_float3(abj4.x, abj4.y, abj4.z);
-      const float3 dn = make_float3(-d.x, -d.y, -d.z), un = make_float3(-u.x, -u.y, -u.z);
-      const PairAdj o = pair_adjoint(K, a.h, a.particle_radius, dn, r2, un, abj, __ldg(a.nu + t), __ldg(a.coh + t),
-                                     m_k, PRk.y, Psum);
-      xb = make_float3(xb.x - o.rb.x, xb.y - o.rb.y, xb.z - o.rb.z);
-      vb = make_float3(vb.x - o.ub.x, vb.y - o.ub.y, vb.z - o.ub.z);
-      Pb += o.pb_sum;
-      Rb += o.rb_j;
+    const float4 vk = a.vs[s];
+    const float m_k = vk.w;
+    const float2 PRk = a.sc2[s];
+    const float nu_k = a.nu[s], coh_k = a.coh[s];
+    float3 xb = make_float3(0.f, 0.f, 0.f), vb = make_float3(0.f, 0.f, 0.f), abk = make_float3(0.f, 0.f, 0.f);
+    if (pfk & PF_DYNAMIC) {
+      integrate_adjoint(walls_of(a.walls, a.g, world_of(xk)), xyz(xk), xyz(vk), ld3(a.accel, i), a.dt, ld3(a.xbo, i),
+                        ld3(a.vbo, i), xb, vb, abk);
+    } else {
+      xb = ld3(a.xbo, i);
+      vb = ld3(a.vbo, i);
     }
+    const Cubic K(a.h);
+    const float h2m = a.h * a.h * kSupportMargin;
+    float Pb = 0.f, Rb = 0.f, nub = 0.f;
+    record_list<false>(a.g, a.xs, (int)s, xk, a.h, h2m, a.L);
+    visit<false, true>(a.g, a.xs, (int)s, xk, a.h, h2m, a.L, true, [&](int t, float4 xj) {
+      const float3 d = make_float3(xk.x - xj.x, xk.y - xj.y, xk.z - xj.z);
+      const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+      if (r2 == 0.f) return;  // the forward skips coincident pairs
+      const float4 vj = __ldg(a.vs + t);
+      const float2 PRj = __ldg(a.sc2 + t);
+      const float3 u = make_float3(vk.x - vj.x, vk.y - vj.y, vk.z - vj.z);
+      const float Psum = PRk.x + PRj.x;
+      if (pfk & PF_DYNAMIC) {  // term of a_k with neighbour j
+        const PairAdj o = pair_adjoint(K, a.h, a.particle_radius, d, r2, u, abk, nu_k, coh_k, vj.w, PRj.y, Psum);
+        xb = make_float3(xb.x + o.rb.x, xb.y + o.rb.y, xb.z + o.rb.z);
+        vb = make_float3(vb.x + o.ub.x, vb.y + o.ub.y, vb.z + o.ub.z);
+        Pb += o.pb_sum;
+        nub += o.nub;
+      }
+      if (pf_of(xj) & PF_DYNAMIC) {  // term of a_j with neighbour k: d_jk = -d, u_jk = -u
+        const float4 abj4 = __ldg(a.ab + t);
+        const float3 abj = make_float3(abj4.x, abj4.y, abj4.z);
+        const float3 dn = make_float3(-d.x, -d.y, -d.z), un = make_float3(-u.x, -u.y, -u.z);
+        const PairAdj o = pair_adjoint(K, a.h, a.particle_radius, dn, r2, un, abj, __ldg(a.nu + t), __ldg(a.coh + t),
+                                       m_k, PRk.y, Psum);
+        xb = make_float3(xb.x - o.rb.x, xb.y - o.rb.y, xb.z - o.rb.z);
+        vb = make_float3(vb.x - o.ub.x, vb.y - o.ub.y, vb.z - o.ub.z);
+        Pb += o.pb_sum;
+        Rb += o.rb_j;
+      }
+    });
+    // P = p / max(rho^2, 1e-6), R = 1 / max(rho, 1e-6), then the EOS
+    const float rho = a.rho[i], p = a.pressure[i];
+    const float rr = rho * rho;
+    const float inv_rr = 1.0f / fmaxf(rr, 1.0e-6f);
+    float rhob = 0.f;
+    if (rr > 1.0e-6f) rhob -= 2.f * Pb * p * inv_rr / rho;
+    if (rho > 1.0e-6f) rhob -= Rb / rr;
+    const float pb = Pb * inv_rr;
+    const float B = a.m.stiffness[i], gam = a.m.exponent[i], rd = a.m.rest_density[i];
+    const float rho0 = fmaxf(rd, 1.0e-6f);
+    const float ratio = rho / rho0;
+    const float pw = powf(ratio, gam);
+    const float p_raw = B * (pw - 1.0f);
+    if (!(a.clamp && p_raw < 0.f) && pb != 0.f) {
+      const float dp_dratio = B * gam * (ratio > 0.f ? pw / ratio : 0.f);
+      rhob += pb * dp_dratio / rho0;
+      if (a.gb_stiffness) a.gb_stiffness[i] += pb * (pw - 1.0f);
+      if (a.gb_rest_density && rd > 1.0e-6f) a.gb_rest_density[i] += -pb * dp_dratio * ratio / rho0;
+    }
+    if (a.gb_viscosity) a.gb_viscosity[i] += nub;
+    a.xr[s] = make_float4(xb.x, xb.y, xb.z, rhob);
+    st3(a.vbi, i, vb);
   });
-  // P = p / max(rho^2, 1e-6), R = 1 / max(rho, 1e-6), then the EOS
-  const float rho = a.rho[i], p = a.pressure[i];
-  const float rr = rho * rho;
-  const float inv_rr = 1.0f / fmaxf(rr, 1.0e-6f);
-  float rhob = 0.f;
-  if (rr > 1.0e-6f) rhob -= 2.f * Pb * p * inv_rr / rho;
-  if (rho > 1.0e-6f) rhob -= Rb / rr;
-  const float pb = Pb * inv_rr;
-  const float B = a.m.stiffness[i], gam = a.m.exponent[i], rd = a.m.rest_density[i];
-  const float rho0 = fmaxf(rd, 1.0e-6f);
-  const float ratio = rho / rho0;
-  const float pw = powf(ratio, gam);
-  const float p_raw = B * (pw - 1.0f);
-  if (!(a.clamp && p_raw < 0.f) && pb != 0.f) {
-    const float dp_dratio = B * gam * (ratio > 0.f ? pw / ratio : 0.f);
-    rhob += pb * dp_dratio / rho0;
-    if (a.gb_stiffness) a.gb_stiffness[i] += pb * (pw - 1.0f);
-    if (a.gb_rest_density && rd > 1.0e-6f) a.gb_rest_density[i] += -pb * dp_dratio * ratio / rho0;
-  }
-  if (a.gb_viscosity) a.gb_viscosity[i] += nub;
-  a.xr[s] = make_float4(xb.x, xb.y, xb.z, rhob);
-  st3(a.vbi, i, vb);
 }
 
 __global__ void FS_NB_BOUNDS k_adj_density(AdjArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const float4 xk = a.xs[s];
-  if (!(pf_of(xk) & PF_ACTIVE)) return;  // written by the force pass
-  const int32_t i = a.g.perm[s];
-  const float4 xr = a.xr[s];
-  const float mv_k = a.mv[s];
-  const Cubic K(a.h);
-  float3 xb = make_float3(xr.x, xr.y, xr.z);
-  const bool lists_ok = lists_usable(a.L);
-  visit<false, false>(a.g, a.xs, (int)s, xk, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok, [&](int t, float4 xj) {
-    const float dx = xk.x - xj.x, dy = xk.y - xj.y, dz = xk.z - xj.z;
-    float r, rinv;
-    r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-    const float w = (xr.w * __ldg(a.mv + t) + __ldg(&a.xr[t].w) * mv_k) * K.grad_scale(r, rinv);
-    xb = make_float3(fmaf(w, dx, xb.x), fmaf(w, dy, xb.y), fmaf(w, dz, xb.z));
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xk = a.xs[s];
+    if (!(pf_of(xk) & PF_ACTIVE)) return;  // written by the force pass
+    const int32_t i = a.g.perm[s];
+    const float4 xr = a.xr[s];
+    const float mv_k = a.mv[s];
+    const Cubic K(a.h);
+    float3 xb = make_float3(xr.x, xr.y, xr.z);
+    const bool lists_ok = lists_usable(a.L);
+    visit<false, false>(a.g, a.xs, (int)s, xk, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok, [&](int t, float4 xj) {
+      const float dx = xk.x - xj.x, dy = xk.y - xj.y, dz = xk.z - xj.z;
+      float r, rinv;
+      r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
+      const float w = (xr.w * __ldg(a.mv + t) + __ldg(&a.xr[t].w) * mv_k) * K.grad_scale(r, rinv);
+      xb = make_float3(fmaf(w, dx, xb.x), fmaf(w, dy, xb.y), fmaf(w, dz, xb.z));
+    });
+    st3(a.xbi, i, xb);
   });
-  st3(a.xbi, i, xb);
 }
 
 
@@ -305,7 +305,7 @@ int fs_wcsph_substep_adjoint(fs_context* c, const fs_model* m, const fs_state* s
   const int64_t n = m->n;
   const float h = p->smoothing_length;
   int rc;
-  if ((rc = grid_build(c, si->particle_q, n, h, st, m->particle_world))) return rc;
+  if ((rc = grid_build(c, si->particle_q, n, h * c->cell_ratio, st, m->particle_world))) return rc;
   AdjArgs a;
   a.g = grid_view(c);
   a.L = nbr_list(c);
@@ -342,11 +342,11 @@ int fs_wcsph_substep_adjoint(fs_context* c, const fs_model* m, const fs_state* s
   }
   {
     PassScope ps_(c, P_ADJ_FORCE, st);
-    k_adj_force<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(a);
+    k_adj_force<<<nb_blocks(c, n), c->nb_block, 0, st>>>(a);
   }
   {
     PassScope ps_(c, P_ADJ_DENSITY, st);
-    k_adj_density<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(a);
+    k_adj_density<<<nb_blocks(c, n), c->nb_block, 0, st>>>(a);
   }
   c->last_stream = st;
   return launch_check("fs_wcsph_substep_adjoint");

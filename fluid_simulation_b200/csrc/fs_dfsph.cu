@@ -64,42 +64,42 @@ struct DensFactorArgs {
 // Records the neighbour lists of this grid (positions stay fixed for the half
 // step, so every later pass of the half reuses them exactly).
 __global__ void FS_NB_BOUNDS k_density_factor(DensFactorArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   lists_recorded(a.L);
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const int32_t i = a.g.perm[s];
-  if (!(pf_of(xi) & PF_ACTIVE)) {
-    a.rho[i] = 0.f;
-    a.factor[i] = 0.f;
-    a.count[i] = 0;
-    a.sc2[s] = make_float2(0.f, 0.f);
-    a.L.cnt[s] = 0;
-    return;
-  }
-  const float h2m = a.h * a.h * kSupportMargin;
-  // the candidate count (no distance test, solver_dfsph.py:163-164) comes from the scan
-  const int cnt = record_list<true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
-  const Cubic K(a.h);
-  float rho = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sq = 0.f;
-  visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    float r, rinv;
-    r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-    rho = fmaf(__ldg(a.mv + t), K.w(r), rho);
-    const float gsc = __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
-    const float gx = gsc * dx, gy = gsc * dy, gz = gsc * dz;
-    sgx += gx;
-    sgy += gy;
-    sgz += gz;
-    sq = fmaf(gx, gx, fmaf(gy, gy, fmaf(gz, gz, sq)));
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    if (!(pf_of(xi) & PF_ACTIVE)) {
+      a.rho[i] = 0.f;
+      a.factor[i] = 0.f;
+      a.count[i] = 0;
+      a.sc2[s] = make_float2(0.f, 0.f);
+      a.L.cnt[s] = 0;
+      return;
+    }
+    const float h2m = a.h * a.h * kSupportMargin;
+    // the candidate count (no distance test, solver_dfsph.py:163-164) comes from the scan
+    const int cnt = record_list<true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
+    const Cubic K(a.h);
+    float rho = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sq = 0.f;
+    visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      float r, rinv;
+      r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
+      rho = fmaf(__ldg(a.mv + t), K.w(r), rho);
+      const float gsc = __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
+      const float gx = gsc * dx, gy = gsc * dy, gz = gsc * dz;
+      sgx += gx;
+      sgy += gy;
+      sgz += gz;
+      sq = fmaf(gx, gx, fmaf(gy, gy, fmaf(gz, gz, sq)));
+    });
+    const float denom = (sgx * sgx + sgy * sgy + sgz * sgz) + sq;
+    const float f = (cnt < a.min_nb || denom < 1.0e-6f) ? 0.f : 1.0f / denom;
+    a.rho[i] = rho;
+    a.factor[i] = f;
+    a.count[i] = cnt;
+    a.sc2[s] = make_float2(rho, f);
   });
-  const float denom = (sgx * sgx + sgy * sgy + sgz * sgz) + sq;
-  const float f = (cnt < a.min_nb || denom < 1.0e-6f) ? 0.f : 1.0f / denom;
-  a.rho[i] = rho;
-  a.factor[i] = f;
-  a.count[i] = cnt;
-  a.sc2[s] = make_float2(rho, f);
 }
 
 // acceleration_non_pressure (178-226) + predict_velocity (230-242).
@@ -118,43 +118,43 @@ struct AccelArgs {
 };
 
 __global__ void FS_NB_BOUNDS k_accel_predict(AccelArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const float4 vi = a.vs[s];
-  const int32_t i = a.g.perm[s];
-  if (!(pf_of(xi) & PF_DYNAMIC)) {
-    st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
-    a.vstar[s] = make_float4(0.f, 0.f, 0.f, vi.w);
-    return;
-  }
-  const float mu10 = 10.f * a.m.viscosity[i];
-  const float coh = a.m.surface_tension[i] / vi.w;
-  const float visc_den_add = 0.01f * (a.h * a.h);
-  const Cubic K(a.h);
-  float ax = 0.f, ay = 0.f, az = 0.f;
-  const bool lists_ok = a.use_lists && lists_usable(a.L);
-  visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                      [&](int t, float4 xj) {
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    if (r2 == 0.f) return;  // zero vector d: every term vanishes
-    const float4 vj = __ldg(a.vs + t);
-    const float rho_j = __ldg(&a.sc2[t].x);
-    float r, rinv;
-    r_and_inv(r2, r, rinv);
-    const float wc = coh * vj.w * K.w(fmaxf(r, a.particle_radius));
-    const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
-    const float visc = mu10 * __fdividef(vj.w, fmaxf(rho_j, 1.0e-6f)) * __fdividef(vdot, r2 + visc_den_add);
-    const float c = fmaf(visc, K.grad_scale(r, rinv), -wc);
-    ax = fmaf(c, dx, ax);
-    ay = fmaf(c, dy, ay);
-    az = fmaf(c, dz, az);
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const float4 vi = a.vs[s];
+    const int32_t i = a.g.perm[s];
+    if (!(pf_of(xi) & PF_DYNAMIC)) {
+      st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
+      a.vstar[s] = make_float4(0.f, 0.f, 0.f, vi.w);
+      return;
+    }
+    const float mu10 = 10.f * a.m.viscosity[i];
+    const float coh = a.m.surface_tension[i] / vi.w;
+    const float visc_den_add = 0.01f * (a.h * a.h);
+    const Cubic K(a.h);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const bool lists_ok = a.use_lists && lists_usable(a.L);
+    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t, float4 xj) {
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (r2 == 0.f) return;  // zero vector d: every term vanishes
+      const float4 vj = __ldg(a.vs + t);
+      const float rho_j = __ldg(&a.sc2[t].x);
+      float r, rinv;
+      r_and_inv(r2, r, rinv);
+      const float wc = coh * vj.w * K.w(fmaxf(r, a.particle_radius));
+      const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+      const float visc = mu10 * __fdividef(vj.w, fmaxf(rho_j, 1.0e-6f)) * __fdividef(vdot, r2 + visc_den_add);
+      const float c = fmaf(visc, K.grad_scale(r, rinv), -wc);
+      ax = fmaf(c, dx, ax);
+      ay = fmaf(c, dy, ay);
+      az = fmaf(c, dz, az);
+    });
+    const float3 g = gravity_of(a.m, i);
+    const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
+    st3(a.accel, i, acc);
+    a.vstar[s] = make_float4(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z, vi.w);
   });
-  const float3 g = gravity_of(a.m, i);
-  const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
-  st3(a.accel, i, acc);
-  a.vstar[s] = make_float4(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z, vi.w);
 }
 
 // ---------------------------------------------------- rate + residual ----
@@ -254,10 +254,9 @@ __device__ bool last_block(uint32_t* ticket) {
 
 __global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
   if (a.ctrl && a.ctrl->done) return;  // uniform across the grid: set by an earlier launch
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double term = 0.0;
+  double term = 0.0;  // this thread's residual terms and dynamic particles
   long long dyn = 0;
-  if (s < a.n) {
+  for_slots(a.n, [&](int64_t s) {
     const float4 xi = a.xs[s];
     const int32_t i = a.g.perm[s];
     const int pf = pf_of(xi);
@@ -286,19 +285,19 @@ __global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
       if (is_dyn) {
         const float err = fmaxf(rs - a.rest_density[i], 0.f);
         kap = fminf((err / (a.dt * a.dt)) * rf.y, a.max_kappa);
-        term = (double)err;
+        term += (double)err;
       }
     } else if (is_dyn) {
       const float dc = fmaxf(d, 0.f);
       kap = fminf((1.0f / a.dt) * dc * rf.x * rf.y, a.max_kappa);
-      term = (double)dc;
+      term += (double)dc;
     }
     if (a.kappa_new) {
       a.kappa_new[s] = kap;
       a.kratio_new[s] = kap / fmaxf(rf.x, 1.0e-6f);
     }
-    dyn = is_dyn ? 1 : 0;
-  }
+    dyn += is_dyn ? 1 : 0;
+  });
   if (!a.ctrl) return;
   block_reduce_store(term, dyn, a.red_part, a.red_cnt);
   if (last_block(&a.ctrl->ticket)) residual_finish(a.ctrl, a.red_part, a.red_cnt, gridDim.x, a.it, a.eta);
@@ -322,33 +321,33 @@ struct CorrectArgs {
 
 __global__ void FS_NB_BOUNDS k_correct(CorrectArgs a) {
   if (a.ctrl && a.ctrl->done) return;
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const int32_t i = a.g.perm[s];
-  if (a.kappa_api) a.kappa_api[i] = a.kappa[s];
-  float4 v = a.vstar[s];
-  if (pf_of(xi) & PF_DYNAMIC) {
-    const Cubic K(a.h);
-    const float ci = a.kratio[s];
-    float dvx = 0.f, dvy = 0.f, dvz = 0.f;
-    const bool lists_ok = a.use_lists && lists_usable(a.L);
-    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                        [&](int t, float4 xj) {
-      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      float r, rinv;
-      r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-      const float c = __ldg(&a.vstar[t].w) * (ci + __ldg(a.kratio + t)) * K.grad_scale(r, rinv);
-      dvx = fmaf(c, dx, dvx);
-      dvy = fmaf(c, dy, dvy);
-      dvz = fmaf(c, dz, dvz);
-    });
-    v.x = v.x - a.dt * dvx;
-    v.y = v.y - a.dt * dvy;
-    v.z = v.z - a.dt * dvz;
-    a.vstar[s] = v;
-  }
-  if (a.vstar_api) st3(a.vstar_api, i, xyz(v));
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    if (a.kappa_api) a.kappa_api[i] = a.kappa[s];
+    float4 v = a.vstar[s];
+    if (pf_of(xi) & PF_DYNAMIC) {
+      const Cubic K(a.h);
+      const float ci = a.kratio[s];
+      float dvx = 0.f, dvy = 0.f, dvz = 0.f;
+      const bool lists_ok = a.use_lists && lists_usable(a.L);
+      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                          [&](int t, float4 xj) {
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        float r, rinv;
+        r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
+        const float c = __ldg(&a.vstar[t].w) * (ci + __ldg(a.kratio + t)) * K.grad_scale(r, rinv);
+        dvx = fmaf(c, dx, dvx);
+        dvy = fmaf(c, dy, dvy);
+        dvz = fmaf(c, dz, dvz);
+      });
+      v.x = v.x - a.dt * dvx;
+      v.y = v.y - a.dt * dvy;
+      v.z = v.z - a.dt * dvz;
+      a.vstar[s] = v;
+    }
+    if (a.vstar_api) st3(a.vstar_api, i, xyz(v));
+  });
 }
 
 // kappa / max(rho, 1e-6) of gathered kappas (warm start, separate pass)
@@ -431,11 +430,11 @@ int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float 
   a.ctrl = ctrl;
   a.red_part = c->red_part;
   a.red_cnt = c->red_cnt;
-  if (ctrl && blocks_for(a.n, kNbBlock) > reduction_blocks(c->capacity))
+  if (ctrl && nb_blocks(c, a.n) > reduction_blocks(c->capacity))
     return set_error(FS_ERR_INVALID, "dfsph rate: reduction buffer too small");
   {
     PassScope ps_(c, P_DFSPH_RATE, st);
-    k_rate<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
+    k_rate<<<nb_blocks(c, a.n), c->nb_block, 0, st>>>(a);
   }
   return launch_check("dfsph rate");
 }
@@ -458,7 +457,7 @@ int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float
   a.ctrl = ctrl;
   {
     PassScope ps_(c, P_DFSPH_CORRECT, st);
-    k_correct<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
+    k_correct<<<nb_blocks(c, a.n), c->nb_block, 0, st>>>(a);
   }
   return launch_check("dfsph correct");
 }
@@ -480,7 +479,7 @@ int run_density_factor(fs_context* c, const fs_model* m, float h, int min_nb, fl
   a.sc2 = c->sc2;
   {
     PassScope ps_(c, P_DFSPH_DENSITY_FACTOR, st);
-    k_density_factor<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
+    k_density_factor<<<nb_blocks(c, a.n), c->nb_block, 0, st>>>(a);
   }
   return launch_check("dfsph density/factor");
 }
@@ -545,7 +544,7 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   aa.vstar = c->vs2;
   {
     PassScope ps_(c, P_DFSPH_ACCEL, st);
-    k_accel_predict<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(aa);
+    k_accel_predict<<<nb_blocks(c, n), c->nb_block, 0, st>>>(aa);
   }
   if ((rc = launch_check("dfsph accel"))) return rc;
   if (p->warm_start) {

@@ -372,6 +372,32 @@ int fs_context_create_worlds(fs_context** out, int64_t capacity, const fs_world_
   return FS_OK;
 }
 
+int fs_context_set_tuning(fs_context* c, const fs_tuning* t) {
+  if (!c || !t) return set_error(FS_ERR_INVALID, "fs_context_set_tuning: null argument");
+  if (t->block_size != 64 && t->block_size != 128 && t->block_size != 256)
+    return set_error(FS_ERR_INVALID, "fs_context_set_tuning: block_size must be 64, 128 or 256 (got %d)",
+                     (int)t->block_size);
+  if (t->particles_per_thread != 1 && t->particles_per_thread != 2 && t->particles_per_thread != 4)
+    return set_error(FS_ERR_INVALID, "fs_context_set_tuning: particles_per_thread must be 1, 2 or 4 (got %d)",
+                     (int)t->particles_per_thread);
+  if (t->cell_ratio != 1.0f && t->cell_ratio != 0.5f)
+    return set_error(FS_ERR_INVALID, "fs_context_set_tuning: cell_ratio must be 1 or 0.5");
+  if (c->worlds && t->cell_ratio != 1.0f)
+    return set_error(FS_ERR_INVALID, "fs_context_set_tuning: batched contexts bin in cells of width h");
+  c->nb_block = t->block_size;
+  c->nb_ppt = t->particles_per_thread;
+  c->cell_ratio = t->cell_ratio;
+  return FS_OK;
+}
+
+int fs_context_get_tuning(const fs_context* c, fs_tuning* t) {
+  if (!c || !t) return set_error(FS_ERR_INVALID, "fs_context_get_tuning: null argument");
+  t->block_size = c->nb_block;
+  t->particles_per_thread = c->nb_ppt;
+  t->cell_ratio = c->cell_ratio;
+  return FS_OK;
+}
+
 int32_t fs_context_worlds(const fs_context* c) { return c ? c->nworlds : -1; }
 int64_t fs_context_cells(const fs_context* c) { return c ? c->ncell : -1; }
 

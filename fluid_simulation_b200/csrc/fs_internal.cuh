@@ -113,6 +113,11 @@ struct fs_context {
   int32_t nworlds = 0;
   float world_cell = 0.f;          // cell width of the world boxes (the solvers' h)
 
+  // launch tuning of the neighbour kernels (fs_context_set_tuning)
+  int32_t nb_block = 128;      // threads per block: 64, 128 or 256
+  int32_t nb_ppt = 1;          // particles per thread: 1, 2 or 4
+  float cell_ratio = 1.f;      // WCSPH grid cell width / h: 1 or 1/2
+
   // instrumentation
   fs::PassTimer timer;
   int64_t launches = 0;  // kernels launched through this context (host count)
@@ -139,6 +144,13 @@ struct DeviceGuard {
 };
 
 inline int blocks_for(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+// Blocks of a neighbour-kernel launch under the context's tuning.
+inline int nb_blocks(const fs_context* c, int64_t n) {
+  const int64_t per = (int64_t)c->nb_block * c->nb_ppt;
+  const int64_t b = (n + per - 1) / per;
+  return (int)(b > 0 ? b : 1);
+}
 
 // Brackets the launches of one pass: counts them and, when the timer is on,
 // records a CUDA event pair around them on the launching stream.
@@ -170,6 +182,15 @@ GridDev grid_view(const fs_context* c);
 
 // DFSPH residual helper shared with the separate-pass entry (fs_dfsph.cu)
 int reduction_blocks(int64_t n);
+
+// Grid-stride loop over cell-sorted slots: thread k of a grid of G threads
+// takes slots k, k + G, ...  Launched with ceil(n / (block * p)) blocks,
+// every thread handles p particles (fs_tuning.particles_per_thread).
+template <class F>
+__device__ __forceinline__ void for_slots(int64_t n, F&& f) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) f(s);
+}
 
 // ----------------------------------------------------------- device math --
 #define FS_DEV __device__ __forceinline__

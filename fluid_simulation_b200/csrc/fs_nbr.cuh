@@ -13,19 +13,11 @@
 
 namespace fs {
 
-constexpr int kNbBlock = 128;  // threads per block of neighbour kernels
-
-// Launch bounds of the neighbour kernels: the minimum number of resident
-// blocks per SM sets the register budget the compiler may use
-// (65536 / (kNbBlock * min blocks)); 0 leaves it to the compiler.
-#ifndef FS_NB_MIN_BLOCKS
-#define FS_NB_MIN_BLOCKS 0
-#endif
-#if FS_NB_MIN_BLOCKS > 0
-#define FS_NB_BOUNDS __launch_bounds__(kNbBlock, FS_NB_MIN_BLOCKS)
-#else
-#define FS_NB_BOUNDS __launch_bounds__(kNbBlock)
-#endif
+// Neighbour kernels are compiled for blocks of up to kNbBlockMax threads;
+// the launch size (64, 128 or 256) and the particles per thread come from
+// the context's tuning (fs_context_set_tuning, chosen by the autotuner).
+constexpr int kNbBlockMax = 256;
+#define FS_NB_BOUNDS __launch_bounds__(kNbBlockMax)
 
 // support test margin: FMA-evaluated r^2 may differ from the individually
 // rounded r^2 by about one ulp; anything the reference counts (r <= h) passes

@@ -15,13 +15,11 @@
 // one binned at build time, queried from the particle's current position.
 #include "fs_nbr.cuh"
 
-// The PBF neighbour kernels run fastest with 8 resident 128-thread blocks
-// per SM (a 64-register budget, no spills): measured 3 % faster per substep
-// on the 401,856-particle dam break than the compiler's own choice
-// (56 registers with spills) and than 6 blocks (85 registers).
-#ifndef FS_NB_BOUNDS_PBF
-#define FS_NB_BOUNDS_PBF __launch_bounds__(kNbBlock, 8)
-#endif
+// The PBF neighbour kernels run fastest with a 64-register budget (1024
+// resident threads per SM, no spills): measured 3 % faster per substep on
+// the 401,856-particle dam break than the compiler's own choice (56
+// registers with spills) and than an 85-register budget.
+#define FS_NB_BOUNDS_PBF __launch_bounds__(kNbBlockMax, 1024 / kNbBlockMax)
 
 namespace fs {
 
@@ -64,30 +62,30 @@ __global__ void FS_NB_BOUNDS_PBF k_density(GridDev g, NbrList L, int record, int
                                                       const float4* __restrict__ xs, const float4* __restrict__ vs,
                                                       const float* __restrict__ mv, float h, float* rho,
                                                       float2* __restrict__ sc2) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (record) lists_recorded(L);
-  if (s >= n) return;
-  const float4 xi = xs[s];
-  const int32_t i = g.perm[s];
-  float acc = 0.f;
-  const float h2m = h * h * kSupportMargin;
-  const Poly6Spiky K(h);
-  auto pair = [&](int t, float4 xj) {
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    acc = fmaf(__ldg(mv + t), K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz))), acc);
-  };
-  if (pf_of(xi) & PF_ACTIVE) {
-    if (record) {
-      record_list<false>(g, xs, (int)s, xi, h, h2m, L);
-      visit<true, true>(g, xs, (int)s, xi, h, h2m, L, true, pair);
-    } else {
-      scan_grid<true>(g, xs, (int)s, xi, h, h2m, pair);
+  for_slots(n, [&](int64_t s) {
+    const float4 xi = xs[s];
+    const int32_t i = g.perm[s];
+    float acc = 0.f;
+    const float h2m = h * h * kSupportMargin;
+    const Poly6Spiky K(h);
+    auto pair = [&](int t, float4 xj) {
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      acc = fmaf(__ldg(mv + t), K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz))), acc);
+    };
+    if (pf_of(xi) & PF_ACTIVE) {
+      if (record) {
+        record_list<false>(g, xs, (int)s, xi, h, h2m, L);
+        visit<true, true>(g, xs, (int)s, xi, h, h2m, L, true, pair);
+      } else {
+        scan_grid<true>(g, xs, (int)s, xi, h, h2m, pair);
+      }
+    } else if (record) {
+      L.cnt[s] = 0;
     }
-  } else if (record) {
-    L.cnt[s] = 0;
-  }
-  rho[i] = acc;
-  sc2[s] = make_float2(acc, vs[s].w / fmaxf(acc, 1.0e-6f));
+    rho[i] = acc;
+    sc2[s] = make_float2(acc, vs[s].w / fmaxf(acc, 1.0e-6f));
+  });
 }
 
 // acceleration_non_pressure (145-189, PBF branches) + apply_non_pressure_prediction
@@ -108,51 +106,51 @@ struct AccelArgs {
 };
 
 __global__ void FS_NB_BOUNDS_PBF k_accel_apply(AccelArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const int32_t i = a.g.perm[s];
-  if (!(pf_of(xi) & PF_DYNAMIC)) {
-    st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
-    a.xs_out[s] = xi;
-    return;
-  }
-  const float4 vi = a.vs[s];
-  const float mu = a.m.viscosity[i];
-  const float gamma = a.m.surface_tension[i];
-  const float coh = gamma / vi.w;
-  const float mu10 = 10.f * mu;
-  const float visc_den_add = 0.01f * (a.h * a.h);
-  const float rp2 = a.particle_radius * a.particle_radius;
-  const Poly6Spiky K(a.h);
-  float ax = 0.f, ay = 0.f, az = 0.f;
-  if (gamma != 0.f || mu != 0.f) {
-    const bool lists_ok = a.use_lists && lists_usable(a.L);
-    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                        [&](int t, float4 xj) {
-      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const float4 vj = __ldg(a.vs + t);
-      float c = 0.f;
-      if (gamma != 0.f) c -= coh * vj.w * K.w_r2(fmaxf(r2, rp2));  // W(max(r, r_p))
-      if (mu != 0.f) {
-        const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
-        if (vdot != 0.f) {
-          float r, rinv;
-          r_and_inv(r2, r, rinv);
-          c += mu10 * __ldg(&a.sc2[t].y) * __fdividef(vdot, r2 + visc_den_add) * K.grad_scale(r, rinv);
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    if (!(pf_of(xi) & PF_DYNAMIC)) {
+      st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
+      a.xs_out[s] = xi;
+      return;
+    }
+    const float4 vi = a.vs[s];
+    const float mu = a.m.viscosity[i];
+    const float gamma = a.m.surface_tension[i];
+    const float coh = gamma / vi.w;
+    const float mu10 = 10.f * mu;
+    const float visc_den_add = 0.01f * (a.h * a.h);
+    const float rp2 = a.particle_radius * a.particle_radius;
+    const Poly6Spiky K(a.h);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (gamma != 0.f || mu != 0.f) {
+      const bool lists_ok = a.use_lists && lists_usable(a.L);
+      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                          [&](int t, float4 xj) {
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float4 vj = __ldg(a.vs + t);
+        float c = 0.f;
+        if (gamma != 0.f) c -= coh * vj.w * K.w_r2(fmaxf(r2, rp2));  // W(max(r, r_p))
+        if (mu != 0.f) {
+          const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+          if (vdot != 0.f) {
+            float r, rinv;
+            r_and_inv(r2, r, rinv);
+            c += mu10 * __ldg(&a.sc2[t].y) * __fdividef(vdot, r2 + visc_den_add) * K.grad_scale(r, rinv);
+          }
         }
-      }
-      ax = fmaf(c, dx, ax);
-      ay = fmaf(c, dy, ay);
-      az = fmaf(c, dz, az);
-    });
-  }
-  st3(a.accel, i, make_float3(ax, ay, az));
-  const float dvx = a.dt * ax, dvy = a.dt * ay, dvz = a.dt * az;
-  float3 p = make_float3(xi.x + a.dt * dvx, xi.y + a.dt * dvy, xi.z + a.dt * dvz);
-  clamp_position(walls_of(a.walls, a.g, world_of(xi)), p);
-  a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
+        ax = fmaf(c, dx, ax);
+        ay = fmaf(c, dy, ay);
+        az = fmaf(c, dz, az);
+      });
+    }
+    st3(a.accel, i, make_float3(ax, ay, az));
+    const float dvx = a.dt * ax, dvy = a.dt * ay, dvz = a.dt * az;
+    float3 p = make_float3(xi.x + a.dt * dvx, xi.y + a.dt * dvy, xi.z + a.dt * dvz);
+    clamp_position(walls_of(a.walls, a.g, world_of(xi)), p);
+    a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
+  });
 }
 
 // compute_pbf_lambda (246-302)
@@ -173,49 +171,49 @@ struct LambdaArgs {
 };
 
 __global__ void FS_NB_BOUNDS_PBF k_lambda(LambdaArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   lists_recorded(a.L);
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const int32_t i = a.g.perm[s];
-  if (!(pf_of(xi) & PF_DYNAMIC)) {
-    a.L.cnt[s] = 0;
-    a.lam_s[s] = 0.f;
-    if (a.lam) a.lam[i] = 0.f;
-    if (a.rho) a.rho[i] = 0.f;
-    if (a.count) a.count[i] = 0;
-    return;
-  }
-  const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
-  const float inv_rho0 = 1.0f / rho0;
-  const Poly6Spiky K(a.h);
-  float rho = 0.f, sq = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-  int cnt = 0;
-  const float h2m = a.h * a.h * kSupportMargin;
-  // records the lists the delta pass of this iteration (same positions) reuses
-  record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
-  visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    if (t != (int)s && exact_lt_h(dx, dy, dz, a.h, K.h2)) ++cnt;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    float r, rinv;
-    r_and_inv(r2, r, rinv);
-    const float mj = __ldg(&a.vs[t].w);
-    rho = fmaf(mj, K.w_r2(r2), rho);
-    const float c = -(mj * inv_rho0) * K.grad_scale(r, rinv);
-    const float gjx = c * dx, gjy = c * dy, gjz = c * dz;
-    sq = fmaf(gjx, gjx, fmaf(gjy, gjy, fmaf(gjz, gjz, sq)));
-    gx -= gjx;
-    gy -= gjy;
-    gz -= gjz;
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    if (!(pf_of(xi) & PF_DYNAMIC)) {
+      a.L.cnt[s] = 0;
+      a.lam_s[s] = 0.f;
+      if (a.lam) a.lam[i] = 0.f;
+      if (a.rho) a.rho[i] = 0.f;
+      if (a.count) a.count[i] = 0;
+      return;
+    }
+    const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
+    const float inv_rho0 = 1.0f / rho0;
+    const Poly6Spiky K(a.h);
+    float rho = 0.f, sq = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    int cnt = 0;
+    const float h2m = a.h * a.h * kSupportMargin;
+    // records the lists the delta pass of this iteration (same positions) reuses
+    record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
+    visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      if (t != (int)s && exact_lt_h(dx, dy, dz, a.h, K.h2)) ++cnt;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float r, rinv;
+      r_and_inv(r2, r, rinv);
+      const float mj = __ldg(&a.vs[t].w);
+      rho = fmaf(mj, K.w_r2(r2), rho);
+      const float c = -(mj * inv_rho0) * K.grad_scale(r, rinv);
+      const float gjx = c * dx, gjy = c * dy, gjz = c * dz;
+      sq = fmaf(gjx, gjx, fmaf(gjy, gjy, fmaf(gjz, gjz, sq)));
+      gx -= gjx;
+      gy -= gjy;
+      gz -= gjz;
+    });
+    sq = fmaf(gx, gx, fmaf(gy, gy, fmaf(gz, gz, sq)));
+    const float ci = fmaxf(rho / rho0 - 1.0f, 0.f);
+    const float l = (a.min_nb > 0 && cnt < a.min_nb) ? 0.f : -ci / (sq + a.eps);
+    a.lam_s[s] = l;
+    if (a.lam) a.lam[i] = l;
+    if (a.rho) a.rho[i] = rho;
+    if (a.count) a.count[i] = cnt;
   });
-  sq = fmaf(gx, gx, fmaf(gy, gy, fmaf(gz, gz, sq)));
-  const float ci = fmaxf(rho / rho0 - 1.0f, 0.f);
-  const float l = (a.min_nb > 0 && cnt < a.min_nb) ? 0.f : -ci / (sq + a.eps);
-  a.lam_s[s] = l;
-  if (a.lam) a.lam[i] = l;
-  if (a.rho) a.rho[i] = rho;
-  if (a.count) a.count[i] = cnt;
 }
 
 // compute_delta_position + compute_scorr (306-350, 91-101), then
@@ -237,49 +235,49 @@ struct DeltaArgs {
 };
 
 __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const int32_t i = a.g.perm[s];
-  if (!(pf_of(xi) & PF_DYNAMIC)) {
-    st3(a.delta_p, i, make_float3(0.f, 0.f, 0.f));
-    if (a.xs_out) a.xs_out[s] = xi;
-    return;
-  }
-  const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
-  const float li = a.lam_s[s];
-  const Poly6Spiky K(a.h);
-  const bool scorr = a.scorr_k != 0.f && !(a.w_dq <= 1.0e-6f);
-  const float inv_wdq = scorr ? 1.0f / a.w_dq : 0.f;
-  float dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
-  const bool lists_ok = a.use_lists && lists_usable(a.L);
-  visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                      [&](int t, float4 xj) {
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    float r, rinv;
-    r_and_inv(r2, r, rinv);
-    float sc = 0.f;
-    if (scorr) sc = -a.scorr_k * powf(K.w_r2(r2) * inv_wdq, a.scorr_n);
-    const float c = (li + __ldg(a.lam_s + t) + sc) * __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
-    dx_ = fmaf(c, dx, dx_);
-    dy_ = fmaf(c, dy, dy_);
-    dz_ = fmaf(c, dz, dz_);
-  });
-  float3 d = make_float3(dx_ / rho0, dy_ / rho0, dz_ / rho0);
-  if (a.max_dp > 0.f) {
-    const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-    if (len > a.max_dp) {
-      const float sc = a.max_dp / fmaxf(len, 1.0e-12f);
-      d = make_float3(d.x * sc, d.y * sc, d.z * sc);
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    if (!(pf_of(xi) & PF_DYNAMIC)) {
+      st3(a.delta_p, i, make_float3(0.f, 0.f, 0.f));
+      if (a.xs_out) a.xs_out[s] = xi;
+      return;
     }
-  }
-  st3(a.delta_p, i, d);
-  if (a.xs_out) {
-    float3 p = make_float3(xi.x + d.x, xi.y + d.y, xi.z + d.z);
-    if (a.clamp) clamp_position(walls_of(a.walls, a.g, world_of(xi)), p);
-    a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
-  }
+    const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
+    const float li = a.lam_s[s];
+    const Poly6Spiky K(a.h);
+    const bool scorr = a.scorr_k != 0.f && !(a.w_dq <= 1.0e-6f);
+    const float inv_wdq = scorr ? 1.0f / a.w_dq : 0.f;
+    float dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
+    const bool lists_ok = a.use_lists && lists_usable(a.L);
+    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t, float4 xj) {
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float r, rinv;
+      r_and_inv(r2, r, rinv);
+      float sc = 0.f;
+      if (scorr) sc = -a.scorr_k * powf(K.w_r2(r2) * inv_wdq, a.scorr_n);
+      const float c = (li + __ldg(a.lam_s + t) + sc) * __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
+      dx_ = fmaf(c, dx, dx_);
+      dy_ = fmaf(c, dy, dy_);
+      dz_ = fmaf(c, dz, dz_);
+    });
+    float3 d = make_float3(dx_ / rho0, dy_ / rho0, dz_ / rho0);
+    if (a.max_dp > 0.f) {
+      const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+      if (len > a.max_dp) {
+        const float sc = a.max_dp / fmaxf(len, 1.0e-12f);
+        d = make_float3(d.x * sc, d.y * sc, d.z * sc);
+      }
+    }
+    st3(a.delta_p, i, d);
+    if (a.xs_out) {
+      float3 p = make_float3(xi.x + d.x, xi.y + d.y, xi.z + d.z);
+      if (a.clamp) clamp_position(walls_of(a.walls, a.g, world_of(xi)), p);
+      a.xs_out[s] = make_float4(p.x, p.y, p.z, xi.w);
+    }
+  });
 }
 
 // update_velocity_from_positions (403-416), cell order; .w keeps the mass
@@ -316,35 +314,35 @@ struct XsphArgs {
 };
 
 __global__ void FS_NB_BOUNDS_PBF k_xsph_final(XsphArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const float4 vi = a.vel[s];
-  const int32_t i = a.g.perm[s];
-  float3 v = xyz(vi);
-  float3 p = xyz(xi);
-  if (a.x_pred_api) st3(a.x_pred_api, i, p);
-  if (pf_of(xi) & PF_DYNAMIC) {
-    if (a.c > 0.f) {
-      const Poly6Spiky K(a.h);
-      float cx = 0.f, cy = 0.f, cz = 0.f;
-      const bool lists_ok = a.use_lists && lists_usable(a.L);
-      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                          [&](int t, float4 xj) {
-        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const float4 vj = __ldg(a.vel + t);
-        // (m_j / max(rho_j, 1e-6)) W(r), the ratio from the final density pass
-        const float w = __ldg(&a.sc2[t].y) * K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-        cx = fmaf(vj.x - vi.x, w, cx);
-        cy = fmaf(vj.y - vi.y, w, cy);
-        cz = fmaf(vj.z - vi.z, w, cz);
-      });
-      v = make_float3(fmaf(a.c, cx, vi.x), fmaf(a.c, cy, vi.y), fmaf(a.c, cz, vi.z));
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const float4 vi = a.vel[s];
+    const int32_t i = a.g.perm[s];
+    float3 v = xyz(vi);
+    float3 p = xyz(xi);
+    if (a.x_pred_api) st3(a.x_pred_api, i, p);
+    if (pf_of(xi) & PF_DYNAMIC) {
+      if (a.c > 0.f) {
+        const Poly6Spiky K(a.h);
+        float cx = 0.f, cy = 0.f, cz = 0.f;
+        const bool lists_ok = a.use_lists && lists_usable(a.L);
+        visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                            [&](int t, float4 xj) {
+          const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+          const float4 vj = __ldg(a.vel + t);
+          // (m_j / max(rho_j, 1e-6)) W(r), the ratio from the final density pass
+          const float w = __ldg(&a.sc2[t].y) * K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+          cx = fmaf(vj.x - vi.x, w, cx);
+          cy = fmaf(vj.y - vi.y, w, cy);
+          cz = fmaf(vj.z - vi.z, w, cz);
+        });
+        v = make_float3(fmaf(a.c, cx, vi.x), fmaf(a.c, cy, vi.y), fmaf(a.c, cz, vi.z));
+      }
+      if (a.bounds) apply_walls(walls_of(a.walls, a.g, world_of(xi)), p, v);
     }
-    if (a.bounds) apply_walls(walls_of(a.walls, a.g, world_of(xi)), p, v);
-  }
-  if (a.x_out) st3(a.x_out, i, p);
-  st3(a.v_out, i, v);
+    if (a.x_out) st3(a.x_out, i, p);
+    st3(a.v_out, i, v);
+  });
 }
 
 __global__ void k_scatter_x(int64_t n, const int32_t* __restrict__ perm, const float4* __restrict__ xs,
@@ -420,7 +418,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   const int use_lists = 1;
   {
     PassScope ps_(c, P_PBF_DENSITY, st);
-    k_density<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(g, L, 1, n, c->xs, c->vs, c->mv, h, so->rho, c->sc2);
+    k_density<<<nb_blocks(c, n), c->nb_block, 0, st>>>(g, L, 1, n, c->xs, c->vs, c->mv, h, so->rho, c->sc2);
   }
   AccelArgs aa;
   aa.g = g;
@@ -439,7 +437,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   aa.xs_out = c->xs2;
   {
     PassScope ps_(c, P_PBF_ACCEL, st);
-    k_accel_apply<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(aa);
+    k_accel_apply<<<nb_blocks(c, n), c->nb_block, 0, st>>>(aa);
   }
   if ((rc = launch_check("pbf accel"))) return rc;
   float4* cur = c->xs2;
@@ -463,7 +461,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     la.count = so->neighbor_count;
     {
       PassScope ps_(c, P_PBF_LAMBDA, st);
-      k_lambda<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(la);
+      k_lambda<<<nb_blocks(c, n), c->nb_block, 0, st>>>(la);
     }
     DeltaArgs da;
     da.g = gi;
@@ -485,7 +483,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     da.xs_out = nxt;
     {
       PassScope ps_(c, P_PBF_DELTA, st);
-      k_delta<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(da);
+      k_delta<<<nb_blocks(c, n), c->nb_block, 0, st>>>(da);
     }
     if ((rc = launch_check("pbf iteration"))) return rc;
     float4* t = cur;
@@ -507,7 +505,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   const GridDev gf = grid_view(c);
   {
     PassScope ps_(c, P_PBF_DENSITY, st);
-    k_density<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(gf, L, 1, n, cur, c->vs, c->mv, h, so->rho, c->sc2);
+    k_density<<<nb_blocks(c, n), c->nb_block, 0, st>>>(gf, L, 1, n, cur, c->vs, c->mv, h, so->rho, c->sc2);
   }
   {
     PassScope ps_(c, P_PBF_VELOCITY, st);
@@ -530,7 +528,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   xa.x_pred_api = x_pred;
   {
     PassScope ps_(c, P_PBF_XSPH, st);
-    k_xsph_final<<<blocks_for(n, kNbBlock), kNbBlock, 0, st>>>(xa);
+    k_xsph_final<<<nb_blocks(c, n), c->nb_block, 0, st>>>(xa);
   }
   c->last_stream = st;
   return launch_check("pbf final");
@@ -544,7 +542,7 @@ int fs_pbf_density(fs_context* c, const fs_model* m, const float* x, float h, fl
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, x, c->xs, c->vs, c->mv,
                                                        c->status, c->nworlds);
-  k_density<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(grid_view(c), nbr_list(c), 0, m->n, c->xs, c->vs, c->mv, h,
+  k_density<<<nb_blocks(c, m->n), c->nb_block, 0, st>>>(grid_view(c), nbr_list(c), 0, m->n, c->xs, c->vs, c->mv, h,
                                                                 rho, c->sc2);
   return launch_check("fs_pbf_density");
 }
@@ -573,7 +571,7 @@ int fs_pbf_lambda(fs_context* c, const fs_model* m, const float* x_pred, const f
   la.lam = pbf_lambda;
   la.rho = rho;
   la.count = neighbor_count;
-  k_lambda<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(la);
+  k_lambda<<<nb_blocks(c, m->n), c->nb_block, 0, st>>>(la);
   return launch_check("fs_pbf_lambda");
 }
 
@@ -606,7 +604,7 @@ int fs_pbf_delta(fs_context* c, const fs_model* m, const float* x_pred, const fl
   da.walls = Walls{};
   da.delta_p = delta_p;
   da.xs_out = nullptr;
-  k_delta<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(da);
+  k_delta<<<nb_blocks(c, m->n), c->nb_block, 0, st>>>(da);
   return launch_check("fs_pbf_delta");
 }
 
@@ -636,7 +634,7 @@ int fs_pbf_xsph(fs_context* c, const fs_model* m, const float* x_pred, const flo
   xa.x_out = nullptr;
   xa.v_out = v_out;
   xa.x_pred_api = nullptr;
-  k_xsph_final<<<blocks_for(m->n, kNbBlock), kNbBlock, 0, st>>>(xa);
+  k_xsph_final<<<nb_blocks(c, m->n), c->nb_block, 0, st>>>(xa);
   return launch_check("fs_pbf_xsph");
 }
 

@@ -63,33 +63,33 @@ struct DensityArgs {
 };
 
 __global__ void FS_NB_BOUNDS k_wcsph_density(DensityArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   lists_recorded(a.L);
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const int32_t i = a.g.perm[s];
-  if (!(pf_of(xi) & PF_ACTIVE)) {
-    a.rho[i] = 0.f;
-    a.pressure[i] = 0.f;
-    a.sc2[s] = make_float2(0.f, 0.f);
-    a.L.cnt[s] = 0;
-    return;
-  }
-  const float h2m = a.h * a.h * kSupportMargin;
-  record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
-  const Cubic K(a.h);
-  float acc = 0.f;
-  visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    float r, rinv;
-    r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-    acc = fmaf(__ldg(a.mv + t), K.w(r), acc);
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const int32_t i = a.g.perm[s];
+    if (!(pf_of(xi) & PF_ACTIVE)) {
+      a.rho[i] = 0.f;
+      a.pressure[i] = 0.f;
+      a.sc2[s] = make_float2(0.f, 0.f);
+      a.L.cnt[s] = 0;
+      return;
+    }
+    const float h2m = a.h * a.h * kSupportMargin;
+    record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
+    const Cubic K(a.h);
+    float acc = 0.f;
+    visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      float r, rinv;
+      r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
+      acc = fmaf(__ldg(a.mv + t), K.w(r), acc);
+    });
+    float p = a.stiffness[i] * (powf(acc / fmaxf(a.rest_density[i], 1.0e-6f), a.exponent[i]) - 1.0f);
+    if (a.clamp) p = fmaxf(p, 0.f);
+    a.rho[i] = acc;
+    a.pressure[i] = p;
+    a.sc2[s] = make_float2(p / fmaxf(acc * acc, 1.0e-6f), 1.0f / fmaxf(acc, 1.0e-6f));
   });
-  float p = a.stiffness[i] * (powf(acc / fmaxf(a.rest_density[i], 1.0e-6f), a.exponent[i]) - 1.0f);
-  if (a.clamp) p = fmaxf(p, 0.f);
-  a.rho[i] = acc;
-  a.pressure[i] = p;
-  a.sc2[s] = make_float2(p / fmaxf(acc * acc, 1.0e-6f), 1.0f / fmaxf(acc, 1.0e-6f));
 }
 
 // --------------------------------------------------------------- force ----
@@ -112,54 +112,54 @@ struct ForceArgs {
 };
 
 __global__ void FS_NB_BOUNDS k_wcsph_force(ForceArgs a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const float4 xi = a.xs[s];
-  const float4 vi = a.vs[s];
-  const int32_t i = a.g.perm[s];
-  if (!(pf_of(xi) & PF_DYNAMIC)) {
-    st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
-    st3(a.v_out, i, xyz(vi));
-    st3(a.x_out, i, xyz(xi));
-    return;
-  }
-  const float dp_i = a.sc2[s].x;
-  const float mu10 = 10.f * a.m.viscosity[i];
-  const float coh = a.m.surface_tension[i] / vi.w;
-  const float visc_den_add = 0.01f * (a.h * a.h);
-  const Cubic K(a.h);
-  float ax = 0.f, ay = 0.f, az = 0.f;
-  const bool lists_ok = a.use_lists && lists_usable(a.L);
-  visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                      [&](int t, float4 xj) {
-    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    if (r2 == 0.f) return;  // coincident particles: every term carries the zero vector d
-    const float4 vj = __ldg(a.vs + t);
-    const float2 rj = __ldg(a.sc2 + t);  // (p_j / rho_j^2, 1 / rho_j)
-    float r, rinv;
-    r_and_inv(r2, r, rinv);
-    const float m_j = vj.w;
-    // cohesion -gamma/m_i m_j W(max(r, r_p)) d
-    const float wc = coh * m_j * K.w(fmaxf(r, a.particle_radius));
-    // viscosity 10 mu (m_j / rho_j) (v_ij . d) / (r^2 + 0.01 h^2) grad W
-    const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
-    const float visc = mu10 * m_j * rj.y * __fdividef(vdot, r2 + visc_den_add);
-    // pressure -m_j (p_i / rho_i^2 + p_j / rho_j^2) grad W
-    const float pres = -m_j * (dp_i + rj.x);
-    const float c = fmaf(visc + pres, K.grad_scale(r, rinv), -wc);
-    ax = fmaf(c, dx, ax);
-    ay = fmaf(c, dy, ay);
-    az = fmaf(c, dz, az);
+  for_slots(a.n, [&](int64_t s) {
+    const float4 xi = a.xs[s];
+    const float4 vi = a.vs[s];
+    const int32_t i = a.g.perm[s];
+    if (!(pf_of(xi) & PF_DYNAMIC)) {
+      st3(a.accel, i, make_float3(0.f, 0.f, 0.f));
+      st3(a.v_out, i, xyz(vi));
+      st3(a.x_out, i, xyz(xi));
+      return;
+    }
+    const float dp_i = a.sc2[s].x;
+    const float mu10 = 10.f * a.m.viscosity[i];
+    const float coh = a.m.surface_tension[i] / vi.w;
+    const float visc_den_add = 0.01f * (a.h * a.h);
+    const Cubic K(a.h);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const bool lists_ok = a.use_lists && lists_usable(a.L);
+    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t, float4 xj) {
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (r2 == 0.f) return;  // coincident particles: every term carries the zero vector d
+      const float4 vj = __ldg(a.vs + t);
+      const float2 rj = __ldg(a.sc2 + t);  // (p_j / rho_j^2, 1 / rho_j)
+      float r, rinv;
+      r_and_inv(r2, r, rinv);
+      const float m_j = vj.w;
+      // cohesion -gamma/m_i m_j W(max(r, r_p)) d
+      const float wc = coh * m_j * K.w(fmaxf(r, a.particle_radius));
+      // viscosity 10 mu (m_j / rho_j) (v_ij . d) / (r^2 + 0.01 h^2) grad W
+      const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+      const float visc = mu10 * m_j * rj.y * __fdividef(vdot, r2 + visc_den_add);
+      // pressure -m_j (p_i / rho_i^2 + p_j / rho_j^2) grad W
+      const float pres = -m_j * (dp_i + rj.x);
+      const float c = fmaf(visc + pres, K.grad_scale(r, rinv), -wc);
+      ax = fmaf(c, dx, ax);
+      ay = fmaf(c, dy, ay);
+      az = fmaf(c, dz, az);
+    });
+    const float3 g = gravity_of(a.m, i);
+    const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
+    st3(a.accel, i, acc);
+    float3 v = make_float3(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z);
+    float3 p = make_float3(xi.x + v.x * a.dt, xi.y + v.y * a.dt, xi.z + v.z * a.dt);
+    apply_walls(walls_of(a.walls, a.g, world_of(xi)), p, v);
+    st3(a.v_out, i, v);
+    st3(a.x_out, i, p);
   });
-  const float3 g = gravity_of(a.m, i);
-  const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
-  st3(a.accel, i, acc);
-  float3 v = make_float3(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z);
-  float3 p = make_float3(xi.x + v.x * a.dt, xi.y + v.y * a.dt, xi.z + v.z * a.dt);
-  apply_walls(walls_of(a.walls, a.g, world_of(xi)), p, v);
-  st3(a.v_out, i, v);
-  st3(a.x_out, i, p);
 }
 
 // (rho, p) of original order -> force-pass ratios in cell order
@@ -199,7 +199,7 @@ int launch_density(fs_context* c, const fs_model* m, float h, int clamp, bool eo
   a.sc2 = c->sc2;
   {
     PassScope ps_(c, P_WCSPH_DENSITY, st);
-    k_wcsph_density<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
+    k_wcsph_density<<<nb_blocks(c, a.n), c->nb_block, 0, st>>>(a);
   }
   return launch_check("wcsph density");
 }
@@ -224,7 +224,7 @@ int launch_force(fs_context* c, const fs_model* m, const fs_wcsph_params* p, flo
   a.v_out = v_out;
   {
     PassScope ps_(c, P_WCSPH_FORCE, st);
-    k_wcsph_force<<<blocks_for(a.n, kNbBlock), kNbBlock, 0, st>>>(a);
+    k_wcsph_force<<<nb_blocks(c, a.n), c->nb_block, 0, st>>>(a);
   }
   return launch_check("wcsph force");
 }
@@ -258,7 +258,7 @@ int fs_wcsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   DeviceGuard dg(c->device);
   cudaStream_t st = (cudaStream_t)stream;
   const float h = p->smoothing_length;
-  if ((rc = grid_build(c, si->particle_q, m->n, h, st, m->particle_world))) return rc;
+  if ((rc = grid_build(c, si->particle_q, m->n, h * c->cell_ratio, st, m->particle_world))) return rc;
   if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
   if ((rc = launch_density(c, m, h, p->clamp_negative_pressure, true, so->rho, so->pressure, st))) return rc;
   return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st, true);

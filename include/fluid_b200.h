@@ -136,6 +136,29 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
 int fs_context_destroy(fs_context* ctx);
 int64_t fs_context_capacity(const fs_context* ctx);
 
+/* Launch tuning of a context's neighbour kernels (no counterpart in the
+ * reference, whose kernels Warp launches one thread per point).  Chosen by
+ * the autotuner (fluid_simulation_b200.autotune) from measured substeps.
+ *   block_size            threads per block: 64, 128 (default) or 256
+ *   particles_per_thread  1 (default), 2 or 4: each thread walks that many
+ *                         cell-sorted particles (grid-stride)
+ *   cell_ratio            WCSPH grid cell width / h: 1 (default, the
+ *                         reference's grid: candidates in its order) or 0.5
+ *                         (125 half-width cells per query instead of 27;
+ *                         same neighbours, sums in another order).  PBF and
+ *                         DFSPH always bin at h: PBF queries the grid from
+ *                         moved positions and DFSPH counts candidates, so
+ *                         the cell width is part of their results.
+ * block_size and particles_per_thread change no result (DFSPH sums its
+ * residual per block, so its last bits follow block_size). */
+typedef struct {
+  int32_t block_size;
+  int32_t particles_per_thread;
+  float cell_ratio;
+} fs_tuning;
+int fs_context_set_tuning(fs_context* ctx, const fs_tuning* tuning);
+int fs_context_get_tuning(const fs_context* ctx, fs_tuning* tuning);
+
 /* `grid.build(points, radius)` (solver_wcsph.py:456, solver_dfsph.py:624,783,
  * solver_pbf.py:737,858): cell keys, stable sort by cell, cell ranges. */
 int fs_grid_build(fs_context* ctx, const float* x, int64_t n, float radius, fs_stream_t stream);
