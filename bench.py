@@ -54,9 +54,9 @@ B_ALG = {
 }
 PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 4090 (performance_summary.json)
 # DRAM bytes (read + write) per particle per launch from one full ncu capture
-# (cold cache), profiles/pbf_dam_401856.md: k_lambda 26.0 MB + 12.4 MB at
+# (cold cache), profiles/pbf_dam_401856.md: k_lambda 25.66 MB + 12.35 MB at
 # 401,856 particles.
-TRAFFIC_PER_PARTICLE = {"pbf_lambda": 38.3e6 / 401856}
+TRAFFIC_PER_PARTICLE = {"pbf_lambda": 38.01e6 / 401856}
 FALLBACK_HBM_GBS = 6650.0
 SUBSTEP_DT = {"pbf": 1.0 / 240.0, "dfsph": 1.0 / 240.0}
 
@@ -464,6 +464,14 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     lib = _lib.load()
+    if args.only:  # one secondary workload by itself (profiling); prints its record, not the bench line
+        flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        if args.only == "adjoint":
+            rec = time_adjoint(dev, flush, reps=1)
+        else:
+            rec = time_batched(args.only.split("_")[1], dev, flush, frames=1, warm=1)
+        print(json.dumps(dict(only=args.only, record=rec)), flush=True)
+        return
 
     model, solver, dt, n, desc = build_workload(args.workload, dev)
     ctx = model.particle_grid._ctx
@@ -685,6 +693,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph"],
+                    help="run one secondary workload alone (profiling); no bench line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
