@@ -46,6 +46,16 @@ class Tuning(C.Structure):
     _fields_ = [("block_size", I32), ("particles_per_thread", I32), ("cell_ratio", F)]
 
 
+class FrameClock(C.Structure):
+    _fields_ = [("remaining", C.c_double), ("dt", F), ("active", I32), ("substeps", I32), ("run_substeps", I32),
+                ("fault", I32), ("maxima", F * 2), ("pad", I32)]
+
+
+class CflRule(C.Structure):
+    _fields_ = [("frame_dt", C.c_double), ("substep_limit", C.c_double), ("method", I32), ("use_accel", I32),
+                ("h", C.c_double), ("sound_speed", C.c_double), ("viscosity", C.c_double), ("spacing", C.c_double)]
+
+
 class Model(C.Structure):
     _fields_ = [("n", I64), ("n_worlds", I32)] + [(k, P) for k in (
         "particle_flags", "particle_mask", "particle_world", "particle_mass", "gravity", "rest_density",
@@ -93,6 +103,12 @@ SIGNATURES = {
     "fs_context_create_worlds": (C.c_int, [C.POINTER(P), I64, C.POINTER(WorldBox), I32, I32]),
     "fs_context_worlds": (I32, [P]),
     "fs_context_set_tuning": (C.c_int, [P, C.POINTER(Tuning)]),
+    "fs_frame_clock_start": (C.c_int, [P, C.c_double, P]),
+    "fs_frame_clock_advance": (C.c_int, [P, C.POINTER(CflRule), P, I64, P, I64, P]),
+    "fs_wcsph_substep_clocked": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
+                                           C.POINTER(WcsphParams), P, P, P]),
+    "fs_dfsph_nonpressure_predict": (C.c_int, [P, C.POINTER(Model), P, P, P, F, F, F, P, P, P]),
+    "fs_pbf_predict": (C.c_int, [P, C.POINTER(Model), P, P, C.POINTER(PbfParams), P, P, P]),
     "fs_context_get_tuning": (C.c_int, [P, C.POINTER(Tuning)]),
     "fs_context_cells": (I64, [P]),
     "fs_grid_build_worlds": (C.c_int, [P, P, P, I64, F, P]),

@@ -26,6 +26,13 @@ __global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_
 
 namespace {
 
+// xyz of a cell-order float4 stream into an original-order [n][3] array
+__global__ void k_scatter_xyz(int64_t n, const int32_t* __restrict__ perm, const float4* __restrict__ in,
+                              float* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) st3(out, perm[s], xyz(in[s]));
+}
+
 // (a[i], b[i]) of original order into cell order
 __global__ void k_gather_pair(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ a,
                               const float* __restrict__ b, float2* __restrict__ out) {
@@ -623,6 +630,41 @@ int fs_dfsph_density_factor(fs_context* c, const fs_model* m, const float* x, fl
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x, x, c->xs, c->vs2, c->mv, c->status, c->nworlds);
   return run_density_factor(c, m, h, min_nb, rho, factor, neighbor_count, st);
+}
+
+int fs_dfsph_nonpressure_predict(fs_context* c, const fs_model* m, const float* x, const float* v, const float* rho,
+                                 float h, float particle_radius, float dt, float* accel, float* v_star,
+                                 fs_stream_t stream) {
+  if (!c || !m || !x || !v || !rho || !accel || !v_star)
+    return set_error(FS_ERR_INVALID, "fs_dfsph_nonpressure_predict: null argument");
+  if (m->n == 0) return FS_OK;
+  if (!m->particle_flags || !m->particle_mass || !m->gravity || m->n_worlds < 1 || !m->viscosity ||
+      !m->surface_tension)
+    return set_error(FS_ERR_INVALID, "fs_dfsph_nonpressure_predict: missing model array");
+  if (c->built_n != m->n) return set_error(FS_ERR_NOGRID, "fs_dfsph_nonpressure_predict: build the grid first");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n = m->n;
+  k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, x, v, c->xs, c->vs, c->mv, c->status,
+                                                    c->nworlds);
+  k_gather_pair<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, rho, nullptr, c->sc2);
+  AccelArgs aa;
+  aa.g = grid_view(c);
+  aa.L = nbr_list(c);
+  aa.use_lists = 0;
+  aa.n = n;
+  aa.xs = c->xs;
+  aa.vs = c->vs;
+  aa.sc2 = c->sc2;
+  aa.m = *m;
+  aa.h = h;
+  aa.particle_radius = particle_radius;
+  aa.dt = dt;
+  aa.accel = accel;
+  aa.vstar = c->vs2;
+  k_accel_predict<<<nb_blocks(c, n), c->nb_block, 0, st>>>(aa);
+  k_scatter_xyz<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->vs2, v_star);
+  return launch_check("fs_dfsph_nonpressure_predict");
 }
 
 int fs_dfsph_divergence(fs_context* c, const fs_model* m, const float* x, const float* v, float h, float* d_rho_dt,

@@ -28,9 +28,9 @@ constexpr int kScanTile = kScanThreads * kScanItems;  // 4096 cells per block
 
 __global__ void k_cell_keys(int64_t n, const float* __restrict__ x, float inv, int dim_x, int dim_y, int dim_z,
                             int rounding, int32_t* __restrict__ key, int32_t* __restrict__ slot,
-                            int32_t* __restrict__ count, uint32_t* status) {
+                            int32_t* __restrict__ count, uint32_t* status, const fs_frame_clock* clock) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || clock_idle(clock)) return;
   const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
   if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(status, FS_STATUS_NONFINITE);
   GridDev g;
@@ -48,9 +48,9 @@ __global__ void k_cell_keys(int64_t n, const float* __restrict__ x, float inv, i
 __global__ void k_cell_keys_worlds(int64_t n, const float* __restrict__ x, const int32_t* __restrict__ world,
                                    const WorldDev* __restrict__ worlds, int nworlds, float inv,
                                    int32_t* __restrict__ key, int32_t* __restrict__ slot,
-                                   int32_t* __restrict__ count, uint32_t* status) {
+                                   int32_t* __restrict__ count, uint32_t* status, const fs_frame_clock* clock) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || clock_idle(clock)) return;
   const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
   if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(status, FS_STATUS_NONFINITE);
   const int w = world[i];
@@ -61,7 +61,9 @@ __global__ void k_cell_keys_worlds(int64_t n, const float* __restrict__ x, const
 }
 
 // phase 1: per-tile sums
-__global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t m, int32_t* __restrict__ part) {
+__global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t m, int32_t* __restrict__ part,
+                              const fs_frame_clock* clock) {
+  if (clock_idle(clock)) return;
   __shared__ int32_t warp_sums[kScanThreads / 32];
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   int32_t s = 0;
@@ -110,7 +112,8 @@ __device__ int32_t block_exclusive_scan(int32_t v, int32_t* total) {
 }
 
 // phase 2: exclusive scan of the tile sums (one block, <= 1024 * 4 tiles)
-__global__ void k_scan_partials(int32_t* part, int nb) {
+__global__ void k_scan_partials(int32_t* part, int nb, const fs_frame_clock* clock) {
+  if (clock_idle(clock)) return;
   constexpr int kItems = 4;
   const int base = threadIdx.x * kItems;
   int32_t v[kItems];
@@ -132,7 +135,8 @@ __global__ void k_scan_partials(int32_t* part, int nb) {
 
 // phase 3: scan inside tiles, offset by the tile prefix; out has m + 1 entries
 __global__ void k_scan_down(const int32_t* __restrict__ in, int64_t m, const int32_t* __restrict__ part,
-                            int32_t* __restrict__ out) {
+                            int32_t* __restrict__ out, const fs_frame_clock* clock) {
+  if (clock_idle(clock)) return;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   int32_t v[kScanItems];
   int32_t s = 0;
@@ -153,16 +157,17 @@ __global__ void k_scan_down(const int32_t* __restrict__ in, int64_t m, const int
 }
 
 __global__ void k_scatter(int64_t n, const int32_t* __restrict__ key, const int32_t* __restrict__ slot,
-                          const int32_t* __restrict__ off, int32_t* __restrict__ tmp) {
+                          const int32_t* __restrict__ off, int32_t* __restrict__ tmp, const fs_frame_clock* clock) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || clock_idle(clock)) return;
   tmp[off[key[i]] + slot[i]] = (int32_t)i;
 }
 
 __global__ void k_rank(int64_t n, const int32_t* __restrict__ key, const int32_t* __restrict__ off,
-                       const int32_t* __restrict__ tmp, int32_t* __restrict__ perm, int32_t* __restrict__ skey) {
+                       const int32_t* __restrict__ tmp, int32_t* __restrict__ perm, int32_t* __restrict__ skey,
+                       const fs_frame_clock* clock) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
+  if (s >= n || clock_idle(clock)) return;
   const int32_t i = tmp[s];
   const int32_t c = key[i];
   const int32_t a = off[c], b = off[c + 1];
@@ -235,7 +240,8 @@ GridDev grid_view(const fs_context* c) {
   return g;
 }
 
-int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st, const int32_t* world) {
+int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st, const int32_t* world,
+               const fs_frame_clock* clock) {
   if (n < 0 || (n > 0 && !x) || !(radius > 0.f)) return set_error(FS_ERR_INVALID, "grid_build: bad arguments");
   if (c->worlds && n > 0 && !world)
     return set_error(FS_ERR_INVALID, "grid_build: a batched context needs particle_world");
@@ -250,17 +256,17 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
   if (rc) return rc;
   if (n > 0 && c->worlds)
     k_cell_keys_worlds<<<blocks_for(n), kBlock, 0, st>>>(n, x, world, c->worlds, c->nworlds, inv, c->key, c->slot,
-                                                         c->cell_count, c->status);
+                                                         c->cell_count, c->status, clock);
   else if (n > 0)
     k_cell_keys<<<blocks_for(n), kBlock, 0, st>>>(n, x, inv, c->grid.dim_x, c->grid.dim_y, c->grid.dim_z,
-                                                   c->grid.rounding, c->key, c->slot, c->cell_count, c->status);
+                                                   c->grid.rounding, c->key, c->slot, c->cell_count, c->status, clock);
   const int nb = scan_blocks(c->ncell);
-  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part);
-  k_scan_partials<<<1, 1024, 0, st>>>(c->scan_part, nb);
-  k_scan_down<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, c->cell_off);
+  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, clock);
+  k_scan_partials<<<1, 1024, 0, st>>>(c->scan_part, nb, clock);
+  k_scan_down<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, c->cell_off, clock);
   if (n > 0) {
-    k_scatter<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->slot, c->cell_off, c->tmp_ids);
-    k_rank<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->cell_off, c->tmp_ids, c->perm, c->skey);
+    k_scatter<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->slot, c->cell_off, c->tmp_ids, clock);
+    k_rank<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->cell_off, c->tmp_ids, c->perm, c->skey, clock);
   }
   rc = launch_check("grid_build");
   if (rc) return rc;

@@ -54,6 +54,55 @@ __global__ void k_check_finite(const float* __restrict__ x, const float* __restr
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicMax(invalid, 1);
 }
 
+__global__ void k_clock_start(fs_frame_clock* c, double frame_dt) {
+  c->remaining = frame_dt;
+  c->substeps = 0;
+  c->active = frame_dt > 1.0e-12 ? 1 : 0;
+  c->dt = 0.f;
+}
+
+// The harness's substep rule (simulation.py:167-182 and the loop of
+// 185-196) on the device, in double precision as the Python harness
+// evaluates it; maxima[] were just reduced from the current state.
+__global__ void k_clock_rule(fs_frame_clock* c, fs_cfl_rule r) {
+  if (c->fault) {
+    c->active = 0;
+    return;
+  }
+  if (!(c->remaining > 1.0e-12)) {
+    c->active = 0;
+    c->dt = 0.f;
+    return;
+  }
+  const bool use_acc = r.method == 0 && r.use_accel && c->run_substeps > 0;
+  const float v2 = c->maxima[0], a2 = use_acc ? c->maxima[1] : 0.f;
+  if (!isfinite(v2) || !isfinite(a2)) {
+    c->fault |= 1;
+    c->active = 0;
+    return;
+  }
+  const double speed = sqrt((double)v2), accel = sqrt((double)a2);
+  double limit = r.substep_limit;
+  if (r.method == 0) {
+    limit = fmin(limit, 0.25 * r.h / (r.sound_speed + speed));
+    if (accel > 0.0) limit = fmin(limit, 0.25 * sqrt(r.h / accel));
+    if (r.viscosity > 0.0) limit = fmin(limit, 0.025 * r.h * r.h / r.viscosity);
+  } else if (speed > 0.0) {
+    limit = fmin(limit, 0.4 * r.spacing / speed);
+  }
+  const double dt = fmin(c->remaining, limit);
+  if (dt < 1.0e-10) {
+    c->fault |= 2;
+    c->active = 0;
+    return;
+  }
+  c->dt = (float)dt;
+  c->active = 1;
+  c->remaining -= dt;
+  c->substeps += 1;
+  c->run_substeps += 1;
+}
+
 }  // namespace
 }  // namespace fs
 
@@ -83,6 +132,26 @@ int fs_check_finite(const float* x, const float* v, int64_t n, const float* rho,
   if (n == 0) return FS_OK;
   k_check_finite<<<blocks_for(n), kBlock, 0, st>>>(x, v, n, rho, nrho, invalid);
   return launch_check("fs_check_finite");
+}
+
+int fs_frame_clock_start(fs_frame_clock* clock, double frame_dt, fs_stream_t stream) {
+  if (!clock || !(frame_dt >= 0.0)) return set_error(FS_ERR_INVALID, "fs_frame_clock_start: bad arguments");
+  k_clock_start<<<1, 1, 0, (cudaStream_t)stream>>>(clock, frame_dt);
+  return launch_check("fs_frame_clock_start");
+}
+
+int fs_frame_clock_advance(fs_frame_clock* clock, const fs_cfl_rule* rule, const float* v, int64_t nv,
+                           const float* accel, int64_t na, fs_stream_t stream) {
+  if (!clock || !rule || nv < 0 || na < 0 || (nv > 0 && !v) || (na > 0 && !accel) ||
+      (rule->method != 0 && rule->method != 1))
+    return set_error(FS_ERR_INVALID, "fs_frame_clock_advance: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = check_cuda(cudaMemsetAsync(clock->maxima, 0, sizeof(clock->maxima), st), "fs_frame_clock_advance: memset");
+  if (rc) return rc;
+  const int64_t m = nv > na ? nv : na;
+  if (m > 0) k_norm_maxima<<<blocks_for(m), kBlock, 0, st>>>(v, nv, accel, na, clock->maxima);
+  k_clock_rule<<<1, 1, 0, st>>>(clock, *rule);
+  return launch_check("fs_frame_clock_advance");
 }
 
 }  // extern "C"

@@ -177,7 +177,13 @@ struct PassScope {
 
 // grid build (fs_grid.cu)
 // world: particle_world of the model (required by batched contexts, unused otherwise)
-int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st, const int32_t* world);
+// clock (optional): a device-side frame clock; its kernels do nothing while
+// clock->active == 0 (the frame is complete).
+int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStream_t st, const int32_t* world,
+               const fs_frame_clock* clock = nullptr);
+
+// Whether a kernel of a clocked substep has work (no clock: always).
+__device__ __forceinline__ bool clock_idle(const fs_frame_clock* clock) { return clock && !clock->active; }
 GridDev grid_view(const fs_context* c);
 
 // DFSPH residual helper shared with the separate-pass entry (fs_dfsph.cu)

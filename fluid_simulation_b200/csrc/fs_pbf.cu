@@ -534,6 +534,20 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   return launch_check("pbf final");
 }
 
+int fs_pbf_predict(fs_context* c, const fs_model* m, const float* x, const float* v, const fs_pbf_params* p,
+                   float* x_pred, float* v_pred, fs_stream_t stream) {
+  if (!c || !m || !x || !v || !p || !x_pred || !v_pred) return set_error(FS_ERR_INVALID, "fs_pbf_predict: null argument");
+  if (m->n == 0) return FS_OK;
+  if (!m->particle_flags || !m->particle_mask || !m->gravity || m->n_worlds < 1)
+    return set_error(FS_ERR_INVALID, "fs_pbf_predict: missing model array");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 2,
+                             p->particle_radius, p->boundary_epsilon);
+  k_predict<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, *m, grid_view(c), x, v, p->dt, w, x_pred, v_pred);
+  return launch_check("fs_pbf_predict");
+}
+
 int fs_pbf_density(fs_context* c, const fs_model* m, const float* x, float h, float* rho, fs_stream_t stream) {
   if (!c || !m || !x || !rho) return set_error(FS_ERR_INVALID, "fs_pbf_density: null argument");
   if (m->n == 0) return FS_OK;

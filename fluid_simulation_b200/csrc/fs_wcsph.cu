@@ -60,9 +60,11 @@ struct DensityArgs {
   float* rho;                 // original order (API)
   float* pressure;            // original order (API)
   float2* sc2;                // cell order
+  const fs_frame_clock* clock;  // clocked substep: nothing to do once the frame is complete
 };
 
 __global__ void FS_NB_BOUNDS k_wcsph_density(DensityArgs a) {
+  if (clock_idle(a.clock)) return;
   lists_recorded(a.L);
   for_slots(a.n, [&](int64_t s) {
     const float4 xi = a.xs[s];
@@ -109,9 +111,12 @@ struct ForceArgs {
   float* accel;
   float* x_out;
   float* v_out;
+  const fs_frame_clock* clock;  // clocked substep: dt from the clock, nothing to do once the frame is complete
 };
 
 __global__ void FS_NB_BOUNDS k_wcsph_force(ForceArgs a) {
+  if (clock_idle(a.clock)) return;
+  const float dt = a.clock ? a.clock->dt : a.dt;
   for_slots(a.n, [&](int64_t s) {
     const float4 xi = a.xs[s];
     const float4 vi = a.vs[s];
@@ -154,8 +159,8 @@ __global__ void FS_NB_BOUNDS k_wcsph_force(ForceArgs a) {
     const float3 g = gravity_of(a.m, i);
     const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
     st3(a.accel, i, acc);
-    float3 v = make_float3(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z);
-    float3 p = make_float3(xi.x + v.x * a.dt, xi.y + v.y * a.dt, xi.z + v.z * a.dt);
+    float3 v = make_float3(vi.x + dt * acc.x, vi.y + dt * acc.y, vi.z + dt * acc.z);
+    float3 p = make_float3(xi.x + v.x * dt, xi.y + v.y * dt, xi.z + v.z * dt);
     apply_walls(walls_of(a.walls, a.g, world_of(xi)), p, v);
     st3(a.v_out, i, v);
     st3(a.x_out, i, p);
@@ -172,6 +177,18 @@ __global__ void k_gather_ratios(int64_t n, const int32_t* __restrict__ perm, con
   out[s] = make_float2(p[i] / fmaxf(r * r, 1.0e-6f), 1.0f / fmaxf(r, 1.0e-6f));
 }
 
+// A clocked substep after its frame is complete: state_out = state_in.
+__global__ void k_idle_copy(int64_t n, const fs_frame_clock* clock, const float* __restrict__ x_in,
+                            const float* __restrict__ v_in, const float* __restrict__ rho_in,
+                            const float* __restrict__ p_in, float* x_out, float* v_out, float* rho_out, float* p_out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !clock_idle(clock)) return;
+  st3(x_out, i, ld3(x_in, i));
+  st3(v_out, i, ld3(v_in, i));
+  if (rho_in && rho_out) rho_out[i] = rho_in[i];
+  if (p_in && p_out) p_out[i] = p_in[i];
+}
+
 int wcsph_gather(fs_context* c, const fs_model* m, const float* x, const float* v, cudaStream_t st) {
   const int64_t n = m->n;
   {
@@ -182,8 +199,9 @@ int wcsph_gather(fs_context* c, const fs_model* m, const float* x, const float* 
 }
 
 int launch_density(fs_context* c, const fs_model* m, float h, int clamp, bool eos, float* rho, float* pressure,
-                   cudaStream_t st) {
+                   cudaStream_t st, const fs_frame_clock* clock = nullptr) {
   DensityArgs a;
+  a.clock = clock;
   a.g = grid_view(c);
   a.L = nbr_list(c);
   a.n = m->n;
@@ -205,8 +223,9 @@ int launch_density(fs_context* c, const fs_model* m, float h, int clamp, bool eo
 }
 
 int launch_force(fs_context* c, const fs_model* m, const fs_wcsph_params* p, float* accel, float* x_out,
-                 float* v_out, cudaStream_t st, bool use_lists) {
+                 float* v_out, cudaStream_t st, bool use_lists, const fs_frame_clock* clock = nullptr) {
   ForceArgs a;
+  a.clock = clock;
   a.g = grid_view(c);
   a.L = nbr_list(c);
   a.use_lists = use_lists ? 1 : 0;
@@ -262,6 +281,33 @@ int fs_wcsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
   if ((rc = launch_density(c, m, h, p->clamp_negative_pressure, true, so->rho, so->pressure, st))) return rc;
   return launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st, true);
+}
+
+int fs_wcsph_substep_clocked(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so,
+                             const fs_wcsph_params* p, float* accel, const fs_frame_clock* clock, fs_stream_t stream) {
+  if (!c || !si || !so || !p || !clock) return set_error(FS_ERR_INVALID, "fs_wcsph_substep_clocked: null argument");
+  int rc = validate_model(m, true);
+  if (rc) return rc;
+  if (m->n == 0) return FS_OK;
+  if (!m->particle_mask || !m->viscosity || !m->surface_tension || !si->particle_q || !si->particle_qd ||
+      !so->particle_q || !so->particle_qd || !so->rho || !so->pressure || !accel)
+    return set_error(FS_ERR_INVALID, "fs_wcsph_substep_clocked: missing array");
+  if (m->n > c->capacity) return set_error(FS_ERR_CAPACITY, "fs_wcsph_substep_clocked: n > capacity");
+  DeviceGuard dg(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const float h = p->smoothing_length;
+  if ((rc = grid_build(c, si->particle_q, m->n, h * c->cell_ratio, st, m->particle_world, clock))) return rc;
+  if ((rc = wcsph_gather(c, m, si->particle_q, si->particle_qd, st))) return rc;
+  if ((rc = launch_density(c, m, h, p->clamp_negative_pressure, true, so->rho, so->pressure, st, clock))) return rc;
+  if ((rc = launch_force(c, m, p, accel, so->particle_q, so->particle_qd, st, true, clock))) return rc;
+  {
+    PassScope ps_(c, P_OTHER, st);
+    k_idle_copy<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, clock, si->particle_q, si->particle_qd, si->rho,
+                                                     si->pressure, so->particle_q, so->particle_qd, so->rho,
+                                                     so->pressure);
+  }
+  c->last_stream = st;
+  return launch_check("fs_wcsph_substep_clocked");
 }
 
 int fs_wcsph_density(fs_context* c, const fs_model* m, const float* x, float h, int32_t clamp_negative, float* rho,

@@ -12,7 +12,12 @@ way with two graphs for the two ping-pong orders
 
 from __future__ import annotations
 
+import ctypes as C
+import math
+
 import torch
+
+from . import _lib
 
 
 class FrameGraph:
@@ -47,3 +52,91 @@ class FrameGraph:
         """One frame (``substeps`` substeps) as one graph launch on the current stream."""
         self.graph.replay()
         return self.result
+
+
+class DeviceFrameLoop:
+    """The WCSPH dam-break frame loop with its substep rule on the device.
+
+    The reference harness (simulation.py:155-196) reads max |v| and max |a|
+    back to the host before every substep to choose its dt.  Here a frame
+    clock in device memory carries the time left in the frame; one CUDA graph
+    records ``graph_substeps`` pairs of [evaluate the rule on the device
+    (fs_frame_clock_advance), clocked substep (fs_wcsph_substep_clocked)],
+    and a frame replays that graph until the clock reports the frame done:
+    one read of the clock per replay instead of one per substep.  Substeps
+    after the end of the frame copy their input through, so the result is
+    always back in ``sim.state_0`` (``graph_substeps`` is even).  The dt
+    sequence, and hence every state, is the one of ``sim.step()``.
+    """
+
+    MAX_SUBSTEPS = 4096  # the harness's own limit per frame
+
+    def __init__(self, sim, graph_substeps: int = 64):
+        if sim.method != "wcsph":
+            raise NotImplementedError("the device-side substep rule drives the WCSPH solver")
+        if graph_substeps < 2 or graph_substeps % 2:
+            raise ValueError("graph_substeps must be even and >= 2")
+        from .solver import _common as cm
+
+        self.sim = sim
+        self.m = int(graph_substeps)
+        model, solver = sim.model, sim.solver
+        dev = model.device
+        n = model.particle_count
+        self.clock = torch.zeros(C.sizeof(_lib.FrameClock), dtype=torch.uint8, device=dev)
+        start = _lib.FrameClock()
+        start.run_substeps = 1 if sim.total_substeps else 0
+        self.clock.copy_(torch.frombuffer(bytearray(bytes(start)), dtype=torch.uint8))
+        mat = sim.material
+        self.rule = _lib.CflRule(sim.frame_dt, sim.frame_dt / sim.substeps, 0, 1, float(solver.smoothing_length),
+                                 math.sqrt(mat["stiffness"] * mat["exponent"] / sim.scene.spec.density),
+                                 float(mat["viscosity"]), float(sim.scene.spacing))
+        self._ms = cm.model_struct(model, wcsph=True)
+        a, b = sim.state_0, sim.state_1
+        self._si = [cm.state_struct(s, n, dev, need=("rho", "pressure")) for s in (a, b)]
+        self._v = [s.particle_qd for s in (a, b)]
+        self._params = solver.params(0.0)
+        self._acc = solver._particle_accel
+        self._ctx = cm.grid_ctx(model, "DeviceFrameLoop")
+        self.stream = torch.cuda.Stream(device=dev)
+        self.graph = torch.cuda.CUDAGraph()
+        lib = _lib.load()
+        self.stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.graph(self.graph, stream=self.stream):
+            st = self.stream.cuda_stream
+            ck = self.clock.data_ptr()
+            for k in range(self.m):
+                i, o = k % 2, 1 - k % 2
+                _lib.check(lib.fs_frame_clock_advance(ck, C.byref(self.rule), self._v[i].data_ptr(), n,
+                                                      self._acc.data_ptr(), n, st), "clock advance")
+                _lib.check(lib.fs_wcsph_substep_clocked(self._ctx, C.byref(self._ms), C.byref(self._si[i]),
+                                                        C.byref(self._si[o]), C.byref(self._params),
+                                                        self._acc.data_ptr(), ck, st), "clocked substep")
+        torch.cuda.current_stream(dev).wait_stream(self.stream)
+        self.replays = 0
+
+    def read_clock(self) -> _lib.FrameClock:
+        return _lib.FrameClock.from_buffer_copy(self.clock.cpu().numpy().tobytes())
+
+    def step(self):
+        """One display frame."""
+        sim = self.sim
+        lib = _lib.load()
+        st = torch.cuda.current_stream(sim.model.device).cuda_stream
+        _lib.check(lib.fs_frame_clock_start(self.clock.data_ptr(), sim.frame_dt, st), "clock start")
+        while True:
+            self.graph.replay()
+            self.replays += 1
+            c = self.read_clock()
+            if c.fault & 1:
+                raise RuntimeError(f"Non-finite velocity or WCSPH acceleration at frame {sim.frame}")
+            if c.fault:
+                raise RuntimeError("CFL step cannot safely complete this frame")
+            if not c.remaining > 1.0e-12:
+                break
+            if c.substeps >= self.MAX_SUBSTEPS:
+                raise RuntimeError("CFL step cannot safely complete this frame")
+        sim.frame += 1
+        sim.sim_time = sim.frame * sim.frame_dt
+        sim.last_substeps = int(c.substeps)
+        sim.total_substeps += int(c.substeps)

@@ -251,6 +251,12 @@ int fs_wcsph_force_integrate(fs_context* ctx, const fs_model* model, const fs_st
 int fs_dfsph_density_factor(fs_context* ctx, const fs_model* model, const float* x, float h,
                             int32_t min_neighbors_for_factor, float* rho, float* factor, int32_t* neighbor_count,
                             fs_stream_t stream);
+/* DFSPH acceleration_non_pressure + predict_velocity (solver_dfsph.py:178-242),
+ * fused: accel [n][3] (gravity included, 0 for non-dynamic particles) and
+ * v_star = v + dt * accel [n][3]; rho [n] is the density of the step. */
+int fs_dfsph_nonpressure_predict(fs_context* ctx, const fs_model* model, const float* x, const float* v,
+                                 const float* rho, float h, float particle_radius, float dt, float* accel,
+                                 float* v_star, fs_stream_t stream);
 /* DFSPH compute_density_change_rate (solver_dfsph.py:246-272). */
 int fs_dfsph_divergence(fs_context* ctx, const fs_model* model, const float* x, const float* v, float h,
                         float* d_rho_dt, fs_stream_t stream);
@@ -262,6 +268,13 @@ int fs_dfsph_correct(fs_context* ctx, const fs_model* model, const float* x, flo
  * max(a - b, 0) (b may be NULL), written as one double to *out (device). */
 int fs_dfsph_residual(fs_context* ctx, const fs_model* model, const float* a, const float* b, double* out,
                       fs_stream_t stream);
+/* PBF predict_velocity_with_gravity + predict_positions + apply_position_bounds
+ * (solver_pbf.py:193-224, 367-399): v_pred = v + dt g, x_pred = x + dt v_pred
+ * clamped into the walls inset by particle_radius + boundary_epsilon (dynamic
+ * particles; the others copy x and v).  Needs no grid; a batched context
+ * takes each particle's walls from its world. */
+int fs_pbf_predict(fs_context* ctx, const fs_model* model, const float* x, const float* v,
+                   const fs_pbf_params* params, float* x_pred, float* v_pred, fs_stream_t stream);
 /* PBF compute_density (poly6, solver_pbf.py:115-141). */
 int fs_pbf_density(fs_context* ctx, const fs_model* model, const float* x, float h, float* rho, fs_stream_t stream);
 /* PBF compute_pbf_lambda (solver_pbf.py:246-302). */
@@ -283,6 +296,47 @@ int fs_norm_maxima(const float* v, int64_t nv, const float* a, int64_t na, float
  * v[n], rho[nrho] is non-finite, else 0. */
 int fs_check_finite(const float* x, const float* v, int64_t n, const float* rho, int64_t nrho, int32_t* invalid,
                     fs_stream_t stream);
+
+/* ---- device-side harness loop (no counterpart in the reference, whose
+ * harness reads the CFL maxima back to the host before every substep:
+ * simulation.py:140-196) -------------------------------------------------
+ * A frame clock in device memory (caller-owned, 32 bytes) carries the time
+ * left in the frame and the dt of the next substep.  fs_frame_clock_advance
+ * evaluates the harness's substep rule on the device (simulation.py:167-182,
+ * in double precision like the Python harness) from max |v|^2 and |a|^2;
+ * fs_wcsph_substep_clocked then runs with that dt, or, once the frame is
+ * complete, copies state_in to state_out.  A frame thus records as a CUDA
+ * graph of [advance, clocked substep] pairs with one read of the clock per
+ * replay instead of one host round trip per substep. */
+typedef struct {
+  double remaining;      /* time left in the frame (s) */
+  float dt;              /* dt of the next substep; 0 once the frame is complete */
+  int32_t active;        /* 1: the next clocked substep runs */
+  int32_t substeps;      /* substeps taken in this frame */
+  int32_t run_substeps;  /* substeps taken since the clock was zeroed (the
+                            acceleration bound applies from the second on) */
+  int32_t fault;         /* sticky: 1 non-finite maxima, 2 dt below 1e-10 */
+  float maxima[2];       /* |v|^2, |a|^2 of the last evaluation */
+  int32_t pad;
+} fs_frame_clock;        /* zero it (e.g. cudaMemset) before the first frame */
+
+typedef struct {
+  double frame_dt;       /* 1 / fps */
+  double substep_limit;  /* frame_dt / base substeps */
+  int32_t method;        /* 0: WCSPH rule (sound speed, acceleration, viscosity), 1: DFSPH rule (0.4 spacing / |v|) */
+  int32_t use_accel;     /* WCSPH: include the acceleration bound (after the first substep of a run) */
+  double h, sound_speed, viscosity, spacing;
+} fs_cfl_rule;
+
+int fs_frame_clock_start(fs_frame_clock* clock, double frame_dt, fs_stream_t stream);
+int fs_frame_clock_advance(fs_frame_clock* clock, const fs_cfl_rule* rule, const float* v, int64_t nv,
+                           const float* accel, int64_t na, fs_stream_t stream);
+/* fs_wcsph_substep at dt = clock->dt; when clock->active == 0 it copies
+ * particle_q, particle_qd (and rho, pressure when both states give them)
+ * from state_in to state_out and leaves accel as it is. */
+int fs_wcsph_substep_clocked(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
+                             const fs_wcsph_params* params, float* accel, const fs_frame_clock* clock,
+                             fs_stream_t stream);
 
 /* ---- instrumentation (no counterpart in the reference, which only times
  * whole frames with wall clocks: examples/dam_break/benchmark.py:63-72) ----

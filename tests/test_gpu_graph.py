@@ -42,3 +42,37 @@ def test_frame_graph_matches_plain_launches(kind, cls, dt, cuda_device):
     assert torch.equal(out.particle_q, a.particle_q)
     assert torch.equal(out.particle_qd, a.particle_qd)
     assert torch.equal(out.sph.rho, a.sph.rho)
+
+
+def test_device_frame_loop_equals_host_loop(cuda_device):
+    """Two WCSPH dam-break frames with the substep rule evaluated on the
+    device (one graph of 16 clocked substeps, replayed until the frame is
+    done) end in the same bits, after the same number of substeps, as the
+    reference harness loop that reads the maxima back before every substep."""
+    from fluid_simulation_b200.dam_break import DamBreakSimulation
+    from fluid_simulation_b200.graph import DeviceFrameLoop
+
+    s = make_scene(10000)
+    host = DamBreakSimulation(s, "wcsph", device=cuda_device)
+    dev = DamBreakSimulation(s, "wcsph", device=cuda_device)
+    loop = DeviceFrameLoop(dev, graph_substeps=16)
+    for _ in range(2):
+        host.step()
+        loop.step()
+        torch.cuda.synchronize()
+        assert dev.last_substeps == host.last_substeps > 16  # several replays per frame
+    assert torch.equal(dev.state_0.particle_q, host.state_0.particle_q)
+    assert torch.equal(dev.state_0.particle_qd, host.state_0.particle_qd)
+    assert torch.equal(dev.state_0.sph.rho, host.state_0.sph.rho)
+    assert dev.total_substeps == host.total_substeps and loop.replays >= 2 * 2
+
+
+def test_device_frame_loop_reports_nonfinite_state(cuda_device):
+    from fluid_simulation_b200.dam_break import DamBreakSimulation
+    from fluid_simulation_b200.graph import DeviceFrameLoop
+
+    sim = DamBreakSimulation(make_scene(3000), "wcsph", device=cuda_device)
+    loop = DeviceFrameLoop(sim, graph_substeps=4)
+    sim.state_0.particle_qd[7, 2] = float("nan")
+    with pytest.raises(RuntimeError, match="Non-finite"):
+        loop.step()

@@ -4,6 +4,8 @@
     bit for bit (same grid, same kernels, same visiting order);
   - fs_dfsph_density_factor at the end-of-step positions reproduces the
     rho / factor / neighbor_count the DFSPH substep leaves in state_out;
+  - fs_dfsph_nonpressure_predict reproduces the substep's acceleration bit
+    for bit; fs_pbf_predict follows its formula and walls;
   - fs_dfsph_divergence, fs_dfsph_correct, fs_dfsph_residual, fs_pbf_density,
     fs_pbf_lambda, fs_pbf_delta and fs_pbf_xsph agree within 1e-5
     norm-relative with an FP64 brute-force restatement of the reference
@@ -254,3 +256,72 @@ def test_pbf_passes_match_fp64(cuda_device):
                                v_out.data_ptr(), stream(dev)), "xsph")
     torch.cuda.synchronize()
     assert rel_err(v_out.cpu().numpy() - v, v_want - v) <= TOL
+
+
+def test_dfsph_nonpressure_predict_reproduces_substep_accel(cuda_device):
+    """fs_dfsph_nonpressure_predict at the step's input positions, with the
+    density of fs_dfsph_density_factor, gives the acceleration the substep
+    reports (solver._particle_accel) bit for bit, and v* = v + dt a."""
+    dev = cuda_device
+    x, v = block(seed=6)
+    n = len(x)
+    m = model_for(SolverDFSPH, x, v, dev)
+    cfg = SolverDFSPH.SphConfig(particle_radius=0.5 * SPACING, particle_length=SPACING, smoothing_length_coff=2.0,
+                                bound_width=0.3, bound_height=0.3, bound_length=0.2)
+    solver = SolverDFSPH(m, cfg)
+    dt = 1.0 / 240.0
+    s_in, s_out = m.state(), m.state()
+    solver.step(s_in, s_out, None, None, dt)
+    lib = _lib.load()
+    ms = cm.model_struct(m)
+    grid = HashGrid(device=dev)
+    grid.build(s_in.particle_q, H)
+    rho = torch.zeros(n, device=dev)
+    fac = torch.zeros(n, device=dev)
+    cnt = torch.zeros(n, dtype=torch.int32, device=dev)
+    _lib.check(lib.fs_dfsph_density_factor(grid._ctx, C.byref(ms), s_in.particle_q.data_ptr(), H,
+                                           cfg.min_neighbors_for_factor, rho.data_ptr(), fac.data_ptr(),
+                                           cnt.data_ptr(), stream(dev)), "density_factor")
+    acc = torch.zeros(n, 3, device=dev)
+    vstar = torch.zeros(n, 3, device=dev)
+    _lib.check(lib.fs_dfsph_nonpressure_predict(grid._ctx, C.byref(ms), s_in.particle_q.data_ptr(),
+                                                s_in.particle_qd.data_ptr(), rho.data_ptr(), H, 0.5 * SPACING, dt,
+                                                acc.data_ptr(), vstar.data_ptr(), stream(dev)), "nonpressure")
+    torch.cuda.synchronize()
+    assert torch.equal(acc, solver._particle_accel)
+    want = s_in.particle_qd.double() + dt * acc.double()
+    assert rel_err(vstar.cpu().numpy() - v, want.cpu().numpy() - v) <= TOL
+
+
+def test_pbf_predict_matches_formula(cuda_device):
+    """v_pred = v + dt g, x_pred = x + dt v_pred, clamped into the walls inset
+    by the radius (solver_pbf.py:193-224, 367-399)."""
+    dev = cuda_device
+    x, v = block(seed=7)
+    v = v * 20.0  # fast enough to cross the walls in one predict
+    n = len(x)
+    m = model_for(SolverPBF, x, v, dev)
+    lib = _lib.load()
+    ms = cm.model_struct(m)
+    grid = HashGrid(device=dev)
+    grid.reserve(n)
+    p = _lib.PbfParams()
+    p.dt, p.particle_radius = 1.0 / 240.0, 0.5 * SPACING
+    p.bound_width, p.bound_height, p.bound_length = 0.2, 0.2, 0.15
+    xt, vt = T(x, dev), T(v, dev)
+    xp = torch.zeros(n, 3, device=dev)
+    vp = torch.zeros(n, 3, device=dev)
+    _lib.check(lib.fs_pbf_predict(grid._ctx, C.byref(ms), xt.data_ptr(), vt.data_ptr(), C.byref(p), xp.data_ptr(),
+                                  vp.data_ptr(), stream(dev)), "predict")
+    torch.cuda.synchronize()
+    dt = np.float64(p.dt)
+    vw = v.astype(np.float64) + dt * np.array([0.0, 0.0, -10.0])
+    xw = x.astype(np.float64) + dt * vw
+    r = np.float64(np.float32(0.5 * SPACING))
+    lo = np.array([-0.2 + r, -0.2 + r, r])
+    hi = np.array([0.2 - r, 0.2 - r, 0.3 - r])
+    clamped = (xw < lo) | (xw > hi)
+    xw = np.clip(xw, lo, hi)
+    assert clamped.any()  # the walls act
+    assert np.abs(vp.cpu().numpy() - vw).max() <= 1e-6 * np.abs(vw).max()
+    assert np.abs(xp.cpu().numpy() - xw).max() <= 1e-6 * np.abs(xw).max()
