@@ -393,6 +393,53 @@ def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
     return rec
 
 
+# -------------------------------------------------- harness frame loop ----
+def time_frame_loop(dev, flush, target=400000, frames=2):
+    """WCSPH dam-break display frames (make_scene(target), CFL substeps of
+    the reference harness) with the host loop (max |v|, |a| read back before
+    every substep, as simulation.py:155-196) against graph.DeviceFrameLoop
+    (the rule on the device, one graph of 64 clocked substeps replayed until
+    the frame is done).  Both run the same frames from the same state; the
+    line reports whether they end in the same bits."""
+    import torch
+    from fluid_simulation_b200.dam_break import DamBreakSimulation
+    from fluid_simulation_b200.graph import DeviceFrameLoop
+    from fluid_simulation_b200.scene import make_scene
+    s = make_scene(target)
+    host = DamBreakSimulation(s, "wcsph", device=dev)
+    devs = DamBreakSimulation(s, "wcsph", device=dev)
+    loop = DeviceFrameLoop(devs, graph_substeps=64)
+    host.step()
+    loop.step()  # first frame: warm-up of both
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        tot, sub = 0.0, 0
+        for _ in range(frames):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+            flush.zero_()
+            torch.cuda.synchronize()
+        return tot
+
+    t_host = timed(host.step)
+    t_dev = timed(loop.step)
+    same = bool(torch.equal(host.state_0.particle_q, devs.state_0.particle_q))
+    n = s.count
+    rec = dict(workload=f"wcsph_dam_frames_{n}", particles=n, frames=frames,
+               substeps_per_frame=host.last_substeps, ms_per_frame_host_loop=round(t_host / frames, 3),
+               ms_per_frame_device_loop=round(t_dev / frames, 3), speedup=round(t_host / t_dev, 3),
+               value=round(n * host.last_substeps * frames / (t_dev * 1e-3), 1), unit="particle-steps/s (device loop)",
+               graph_replays=loop.replays, final_state_bit_identical=same, total_substeps=int(host.total_substeps))
+    del host, devs, loop
+    torch.cuda.empty_cache()
+    return rec
+
+
 # --------------------------------------------------------------- clocks ----
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -468,6 +515,8 @@ def run_ours(args):
         flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         if args.only == "adjoint":
             rec = time_adjoint(dev, flush, reps=1)
+        elif args.only == "frames":
+            rec = [time_frame_loop(dev, flush), time_frame_loop(dev, flush, target=50000, frames=3)]
         else:
             rec = time_batched(args.only.split("_")[1], dev, flush, frames=1, warm=1)
         print(json.dumps(dict(only=args.only, record=rec)), flush=True)
@@ -612,6 +661,9 @@ def run_ours(args):
     if world == 1 and not args.no_secondary and not args.no_batched:
         for kind in ("pbf", "wcsph"):
             secondary[f"batched_{kind}_256"] = time_batched(kind, dev, flush)
+    if world == 1 and not args.no_secondary:
+        secondary["wcsph_dam_frames_401856"] = time_frame_loop(dev, flush)
+        secondary["wcsph_dam_frames_50232"] = time_frame_loop(dev, flush, target=50000, frames=3)
     if world == 1 and not args.no_secondary and not args.no_adjoint:
         secondary["adjoint_wcsph_50232"] = time_adjoint(dev, flush)
         secondary["batched_adjoint_wcsph_256"] = time_adjoint(dev, flush, batched=True)
@@ -693,7 +745,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph"],
+    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "frames"],
                     help="run one secondary workload alone (profiling); no bench line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
