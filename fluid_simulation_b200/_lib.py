@@ -104,6 +104,7 @@ SIGNATURES = {
     "fs_context_worlds": (I32, [P]),
     "fs_context_set_tuning": (C.c_int, [P, C.POINTER(Tuning)]),
     "fs_frame_clock_start": (C.c_int, [P, C.c_double, P]),
+    "fs_frame_metrics": (C.c_int, [P, P, P, I64, P, P, I64, I64, P, P]),
     "fs_frame_clock_advance": (C.c_int, [P, C.POINTER(CflRule), P, I64, P, I64, P]),
     "fs_wcsph_substep_clocked": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
                                            C.POINTER(WcsphParams), P, P, P]),

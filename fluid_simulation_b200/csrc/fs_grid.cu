@@ -433,6 +433,7 @@ static int context_alloc(fs_context* c, int64_t capacity, int64_t ncell) {
       {(void**)&c->tile_stats, sizeof(unsigned long long) * 8},
       {(void**)&c->nb_idx, sizeof(int32_t) * kNbMax * cap},  {(void**)&c->nb_cnt, sizeof(int32_t) * cap},
       {(void**)&c->nb_ctl, sizeof(ListCtl)},
+      {(void**)&c->metrics, metrics_scratch_bytes(cap)},
   };
   for (auto& a : allocs) {
     cudaError_t e = cudaMalloc(a.p, a.bytes);
@@ -461,7 +462,7 @@ int fs_context_destroy(fs_context* c) {
   timer_free(c->timer);
   void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
                 c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
-                c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds};
+                c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds, c->metrics};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete c;

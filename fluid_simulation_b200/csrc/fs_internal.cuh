@@ -113,6 +113,9 @@ struct fs_context {
   int32_t nworlds = 0;
   float world_cell = 0.f;          // cell width of the world boxes (the solvers' h)
 
+  // frame metrics scratch (fs_metrics.cu)
+  void* metrics = nullptr;
+
   // launch tuning of the neighbour kernels (fs_context_set_tuning)
   int32_t nb_block = 128;      // threads per block: 64, 128 or 256
   int32_t nb_ppt = 1;          // particles per thread: 1, 2 or 4
@@ -188,6 +191,9 @@ GridDev grid_view(const fs_context* c);
 
 // DFSPH residual helper shared with the separate-pass entry (fs_dfsph.cu)
 int reduction_blocks(int64_t n);
+
+// bytes of the frame-metrics scratch of a context (fs_metrics.cu)
+size_t metrics_scratch_bytes(int64_t capacity);
 
 // Grid-stride loop over cell-sorted slots: thread k of a grid of G threads
 // takes slots k, k + G, ...  Launched with ceil(n / (block * p)) blocks,

@@ -45,6 +45,28 @@ def solver_config(method, scene: ParticleScene, *, wcsph_smoothing_length_coff=2
     raise ValueError(f"unknown method {method!r} (the particle path provides wcsph, dfsph, pbf)")
 
 
+def percentile99_ranks(n: int):
+    """Sorted positions whose values numpy.percentile(a, 99) interpolates
+    for a float32 array of n values: q = float32(0.99), index (n - 1) q in
+    float32 (numpy 2 keeps the array's dtype)."""
+    q = np.float32(99) / np.float32(100)
+    virtual = np.float32(n - 1) * q
+    k = int(np.floor(virtual))
+    return k, min(k + 1, n - 1)
+
+
+def percentile99(a: float, b: float, n: int) -> np.float32:
+    """numpy.percentile(x, 99) of a float32 array of n values from its two
+    order statistics a (k-th) and b ((k+1)-th), numpy's linear method in
+    float32: a + (b - a) g, or b - (b - a)(1 - g) for g >= 0.5."""
+    q = np.float32(99) / np.float32(100)
+    virtual = np.float32(n - 1) * q
+    g = np.float32(virtual - np.float32(np.floor(virtual)))
+    a, b = np.float32(a), np.float32(b)
+    d = np.float32(b - a)
+    return np.float32(b - d * (np.float32(1) - g)) if g >= 0.5 else np.float32(a + d * g)
+
+
 def material(method, scene, wcsph_stiffness=250000.0, wcsph_viscosity=1.0e-6):
     """simulation.py:84-91."""
     m = {"rest_density": scene.spec.density, "surface_tension": 0.0, "viscosity": 1.0e-6}
@@ -89,6 +111,7 @@ class DamBreakSimulation:
         self._norm_maxima = torch.zeros(2, dtype=torch.float32, device=dev)
         self._invalid_state = torch.zeros(1, dtype=torch.int32, device=dev)
         self._host2 = torch.zeros(2, dtype=torch.float32).pin_memory() if dev.type == "cuda" else None
+        self._metrics = None
         del n
 
     @property
@@ -154,7 +177,46 @@ class DamBreakSimulation:
         self.total_substeps += 1
 
     def metrics(self):
-        """simulation.py:198-225."""
+        """simulation.py:198-225, reduced on the device (fs_frame_metrics):
+        14 doubles come back instead of every particle's x, v, rho and p.
+        Minima, maxima, the speed maximum and the density percentile equal
+        the numpy reductions of ``metrics_host`` exactly; the means are
+        double-precision sums (numpy sums float32 pairwise), equal to about
+        1e-7 relative."""
+        s = self.state_0
+        n = s.particle_q.shape[0]
+        with_sph = bool(self.frame)
+        rho = s.sph.rho if with_sph else None
+        pressure = s.sph.pressure if with_sph and self.method == "wcsph" else None
+        nr = n if with_sph else 0
+        k, k1 = percentile99_ranks(nr) if nr else (0, 0)
+        if self._metrics is None:
+            self._metrics = torch.zeros(14, dtype=torch.float64, device=self.model.device)
+        _lib.check(_lib.load().fs_frame_metrics(
+            self.model.particle_grid._ctx, s.particle_q.data_ptr(), s.particle_qd.data_ptr(), n,
+            rho.data_ptr() if rho is not None else None, pressure.data_ptr() if pressure is not None else None, nr, k,
+            self._metrics.data_ptr(), self._stream), "frame metrics")
+        o = self._metrics.tolist()
+        if o[0]:
+            raise RuntimeError(f"Non-finite particle state at frame {self.frame}")
+        result = dict(frame=self.frame, simulation_time=self.sim_time, substeps=self.last_substeps,
+                      total_substeps=self.total_substeps, finite=True, speed_max=o[3] if n else 0.0,
+                      height_mean=o[4], height_min=o[5], height_max=o[6])
+        if with_sph:
+            if o[1]:
+                raise RuntimeError("Non-finite density")
+            result.update(density_mean=o[7], density_min=o[8], density_max=o[9])
+            if self.method == "wcsph":
+                if o[2]:
+                    raise RuntimeError("Non-finite pressure")
+                p99 = float(percentile99(o[10], o[11], nr))
+                result.update(density_p99=p99,
+                              density_compression_p99=max(0.0, p99 / self.scene.spec.density - 1.0),
+                              pressure_min=o[12], pressure_max=o[13])
+        return result
+
+    def metrics_host(self):
+        """simulation.py:198-225 with numpy on host copies (the reference's way)."""
         x, v = self.state_0.particle_q.cpu().numpy(), self.state_0.particle_qd.cpu().numpy()
         finite = bool(np.isfinite(x).all() and np.isfinite(v).all())
         if not finite:
@@ -196,4 +258,5 @@ class DamBreakSimulation:
                     solver_execution="plain launches")
 
 
-__all__ = ["DamBreakSimulation", "SOLVERS", "solver_config", "material", "ModelBuilder", "Axis", "C"]
+__all__ = ["DamBreakSimulation", "SOLVERS", "solver_config", "material", "percentile99", "percentile99_ranks",
+           "ModelBuilder", "Axis", "C"]

@@ -338,6 +338,18 @@ int fs_wcsph_substep_clocked(fs_context* ctx, const fs_model* model, const fs_st
                              const fs_wcsph_params* params, float* accel, const fs_frame_clock* clock,
                              fs_stream_t stream);
 
+/* Frame metrics of the dam-break harness (simulation.py:198-225) reduced on
+ * the device into out[14] (device doubles): [0] non-finite x or v, [1]
+ * non-finite rho, [2] non-finite pressure (1/0), [3] max |v| (float32 norm,
+ * as numpy.linalg.norm), [4..6] mean / min / max of z, [7..9] mean / min /
+ * max of rho, [10] the k-th and [11] the (k+1)-th smallest rho (the (k)-th
+ * again when k = nrho - 1: the percentile's interpolation ends), [12..13]
+ * min / max of pressure (NULL pressure: 0).  Minima, maxima and the order
+ * statistics are exact; means are double sums in a fixed order.  Uses the
+ * context's scratch (n, nrho <= capacity); no grid is needed. */
+int fs_frame_metrics(fs_context* ctx, const float* x, const float* v, int64_t n, const float* rho,
+                     const float* pressure, int64_t nrho, int64_t k, double* out, fs_stream_t stream);
+
 /* ---- instrumentation (no counterpart in the reference, which only times
  * whole frames with wall clocks: examples/dam_break/benchmark.py:63-72) ----
  * Per-pass CUDA-event timer: while enabled, every pass launched through the

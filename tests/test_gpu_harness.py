@@ -148,3 +148,38 @@ def test_multi_frame_statistics_track_oracle(method, cuda_device):
     assert abs(ke_g - ke_c) <= 1e-3 * ke_c
     for q in (1, 50, 99):
         assert abs(np.percentile(rho_g, q) - np.percentile(rho_c, q)) <= 1e-3 * 1000.0
+
+
+@pytest.mark.parametrize("method", ["wcsph", "pbf", "dfsph"])
+def test_device_metrics_equal_numpy_metrics(method, cuda_device):
+    """fs_frame_metrics against the reference's numpy reductions on the same
+    state: minima, maxima, speed maximum and the density percentile exact,
+    means to 1e-6 relative."""
+    from fluid_simulation_b200.dam_break import DamBreakSimulation
+    from fluid_simulation_b200.scene import make_scene
+
+    sim = DamBreakSimulation(make_scene(20000), method, device=cuda_device)
+    for frame in range(2):
+        dev, host = sim.metrics(), sim.metrics_host()
+        assert set(dev) == set(host)
+        for k, want in host.items():
+            got = dev[k]
+            if k.endswith("_mean"):
+                assert abs(got - want) <= 1e-6 * abs(want), k
+            else:
+                assert got == want, (k, got, want)
+        sim.step()
+
+
+def test_device_metrics_report_nonfinite_state(cuda_device):
+    from fluid_simulation_b200.dam_break import DamBreakSimulation
+    from fluid_simulation_b200.scene import make_scene
+
+    sim = DamBreakSimulation(make_scene(3000), "wcsph", device=cuda_device)
+    sim.step()
+    sim.state_0.sph.pressure[5] = float("inf")
+    with pytest.raises(RuntimeError, match="Non-finite pressure"):
+        sim.metrics()
+    sim.state_0.particle_q[3, 1] = float("nan")
+    with pytest.raises(RuntimeError, match="Non-finite particle state"):
+        sim.metrics()
