@@ -57,6 +57,15 @@ PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 40
 # (cold cache), profiles/pbf_dam_401856.md: k_lambda 25.66 MB + 12.35 MB at
 # 401,856 particles.
 TRAFFIC_PER_PARTICLE = {"pbf_lambda": 38.01e6 / 401856}
+# Warp instructions per particle per launch from the same captures
+# (profiles/pbf_dam_401856.md, profiles/wcsph_bcc_524k.md,
+# profiles/dfsph_dam_401856.md): the neighbour passes are bound by
+# instruction issue, so the bench reports the issue rate beside the HBM
+# roofline.  Issue peak = 148 SMs x 4 schedulers x 1 warp instruction per
+# cycle at the SM clock sampled during the timed region.
+WARP_INST_PER_PARTICLE = {"pbf_lambda": 82.78e6 / 401856, "pbf_delta": 24.36e6 / 401856,
+                          "wcsph_density": 120.0e6 / 524288, "wcsph_force": 49.47e6 / 524288,
+                          "dfsph_density_factor": 92.96e6 / 401856, "dfsph_rate": 26.68e6 / 401856}
 FALLBACK_HBM_GBS = 6650.0
 SUBSTEP_DT = {"pbf": 1.0 / 240.0, "dfsph": 1.0 / 240.0}
 
@@ -394,8 +403,8 @@ def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
 
 
 # -------------------------------------------------- harness frame loop ----
-def time_frame_loop(dev, flush, target=400000, frames=2):
-    """WCSPH dam-break display frames (make_scene(target), CFL substeps of
+def time_frame_loop(dev, flush, target=400000, frames=2, method="wcsph"):
+    """WCSPH or DFSPH dam-break display frames (make_scene(target), CFL substeps of
     the reference harness) with the host loop (max |v|, |a| read back before
     every substep, as simulation.py:155-196) against graph.DeviceFrameLoop
     (the rule on the device, one graph of 64 clocked substeps replayed until
@@ -406,9 +415,9 @@ def time_frame_loop(dev, flush, target=400000, frames=2):
     from fluid_simulation_b200.graph import DeviceFrameLoop
     from fluid_simulation_b200.scene import make_scene
     s = make_scene(target)
-    host = DamBreakSimulation(s, "wcsph", device=dev)
-    devs = DamBreakSimulation(s, "wcsph", device=dev)
-    loop = DeviceFrameLoop(devs, graph_substeps=64)
+    host = DamBreakSimulation(s, method, device=dev)
+    devs = DamBreakSimulation(s, method, device=dev)
+    loop = DeviceFrameLoop(devs, graph_substeps=64 if method == "wcsph" else 8)
     host.step()
     loop.step()  # first frame: warm-up of both
     torch.cuda.synchronize()
@@ -430,7 +439,7 @@ def time_frame_loop(dev, flush, target=400000, frames=2):
     t_dev = timed(loop.step)
     same = bool(torch.equal(host.state_0.particle_q, devs.state_0.particle_q))
     n = s.count
-    rec = dict(workload=f"wcsph_dam_frames_{n}", particles=n, frames=frames,
+    rec = dict(workload=f"{method}_dam_frames_{n}", particles=n, frames=frames,
                substeps_per_frame=host.last_substeps, ms_per_frame_host_loop=round(t_host / frames, 3),
                ms_per_frame_device_loop=round(t_dev / frames, 3), speedup=round(t_host / t_dev, 3),
                value=round(n * host.last_substeps * frames / (t_dev * 1e-3), 1), unit="particle-steps/s (device loop)",
@@ -516,7 +525,8 @@ def run_ours(args):
         if args.only == "adjoint":
             rec = time_adjoint(dev, flush, reps=1)
         elif args.only == "frames":
-            rec = [time_frame_loop(dev, flush), time_frame_loop(dev, flush, target=50000, frames=3)]
+            rec = [time_frame_loop(dev, flush), time_frame_loop(dev, flush, target=50000, frames=3),
+                   time_frame_loop(dev, flush, frames=3, method="dfsph")]
         else:
             rec = time_batched(args.only.split("_")[1], dev, flush, frames=1, warm=1)
         print(json.dumps(dict(only=args.only, record=rec)), flush=True)
@@ -589,6 +599,15 @@ def run_ours(args):
                     traffic=(round(TRAFFIC_PER_PARTICLE[dom] * n) if dom in TRAFFIC_PER_PARTICLE else None),
                     bytes_per_launch=bpl,
                     share_of_step=round(passes[dom]["ms_total"] / max(step_ms, 1e-9), 3))
+    if dom in WARP_INST_PER_PARTICLE:
+        inst = WARP_INST_PER_PARTICLE[dom] * n
+        mhz = (clk or {}).get("sm_mhz") or 1965.0
+        peak_inst = 148 * 4 * mhz * 1e6
+        rate = inst / (passes[dom]["ms_avg"] * 1e-3)
+        roofline["issue"] = dict(kernel=dom, warp_instructions_per_launch=round(inst),
+                                 achieved_warp_inst_per_s=round(rate), peak_warp_inst_per_s=round(peak_inst),
+                                 frac=round(rate / peak_inst, 4), sm_mhz=mhz,
+                                 source="warp instructions per particle from the committed ncu capture")
     all_passes_b = sum(B_ALG.get(k, 0) * n * v["launches"] for k, v in passes.items())
     step_roofline = dict(algorithmic_bytes_per_step=all_passes_b / K, achieved_gbs=round(
         all_passes_b / (step_ms * 1e-3) / 1e9, 1), frac=round(all_passes_b / (step_ms * 1e-3) / 1e9 / peak, 4))
@@ -664,6 +683,7 @@ def run_ours(args):
     if world == 1 and not args.no_secondary:
         secondary["wcsph_dam_frames_401856"] = time_frame_loop(dev, flush)
         secondary["wcsph_dam_frames_50232"] = time_frame_loop(dev, flush, target=50000, frames=3)
+        secondary["dfsph_dam_frames_401856"] = time_frame_loop(dev, flush, frames=3, method="dfsph")
     if world == 1 and not args.no_secondary and not args.no_adjoint:
         secondary["adjoint_wcsph_50232"] = time_adjoint(dev, flush)
         secondary["batched_adjoint_wcsph_256"] = time_adjoint(dev, flush, batched=True)

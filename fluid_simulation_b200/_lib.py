@@ -108,6 +108,8 @@ SIGNATURES = {
     "fs_frame_clock_advance": (C.c_int, [P, C.POINTER(CflRule), P, I64, P, I64, P]),
     "fs_wcsph_substep_clocked": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
                                            C.POINTER(WcsphParams), P, P, P]),
+    "fs_dfsph_substep_clocked": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
+                                           C.POINTER(DfsphParams), P, P, P]),
     "fs_dfsph_nonpressure_predict": (C.c_int, [P, C.POINTER(Model), P, P, P, F, F, F, P, P, P]),
     "fs_pbf_predict": (C.c_int, [P, C.POINTER(Model), P, P, C.POINTER(PbfParams), P, P, P]),
     "fs_context_get_tuning": (C.c_int, [P, C.POINTER(Tuning)]),

@@ -66,11 +66,13 @@ struct DensFactorArgs {
   float* factor;
   int32_t* count;
   float2* sc2;       // (rho, factor) cell order
+  const fs_frame_clock* clock;  // clocked substep: nothing to do once the frame is complete
 };
 
 // Records the neighbour lists of this grid (positions stay fixed for the half
 // step, so every later pass of the half reuses them exactly).
 __global__ void FS_NB_BOUNDS k_density_factor(DensFactorArgs a) {
+  if (clock_idle(a.clock)) return;
   lists_recorded(a.L);
   for_slots(a.n, [&](int64_t s) {
     const float4 xi = a.xs[s];
@@ -122,9 +124,12 @@ struct AccelArgs {
   float h, particle_radius, dt;
   float* accel;
   float4* vstar;     // cell order (v*, mass)
+  const fs_frame_clock* clock;
 };
 
 __global__ void FS_NB_BOUNDS k_accel_predict(AccelArgs a) {
+  if (clock_idle(a.clock)) return;
+  const float dt = a.clock ? a.clock->dt : a.dt;
   for_slots(a.n, [&](int64_t s) {
     const float4 xi = a.xs[s];
     const float4 vi = a.vs[s];
@@ -160,7 +165,7 @@ __global__ void FS_NB_BOUNDS k_accel_predict(AccelArgs a) {
     const float3 g = gravity_of(a.m, i);
     const float3 acc = make_float3(ax + g.x, ay + g.y, az + g.z);
     st3(a.accel, i, acc);
-    a.vstar[s] = make_float4(vi.x + a.dt * acc.x, vi.y + a.dt * acc.y, vi.z + a.dt * acc.z, vi.w);
+    a.vstar[s] = make_float4(vi.x + dt * acc.x, vi.y + dt * acc.y, vi.z + dt * acc.z, vi.w);
   });
 }
 
@@ -187,6 +192,7 @@ struct RateArgs {
   DfsphDev* ctrl;           // null: separate-pass use, no residual
   double* red_part;
   int64_t* red_cnt;
+  const fs_frame_clock* clock;
 };
 
 __device__ void residual_finish(DfsphDev* ctrl, const double* part, const int64_t* cntp, int nblk, int it,
@@ -261,6 +267,8 @@ __device__ bool last_block(uint32_t* ticket) {
 
 __global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
   if (a.ctrl && a.ctrl->done) return;  // uniform across the grid: set by an earlier launch
+  if (clock_idle(a.clock)) return;     // uniform: the frame is complete
+  const float dt = a.clock ? a.clock->dt : a.dt;
   double term = 0.0;  // this thread's residual terms and dynamic particles
   long long dyn = 0;
   for_slots(a.n, [&](int64_t s) {
@@ -287,16 +295,16 @@ __global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
     const bool is_dyn = (pf & PF_DYNAMIC) != 0;
     float kap = 0.f;
     if (a.mode == 0) {
-      const float rs = (pf & PF_ACTIVE) ? rf.x + a.dt * d : 0.f;
+      const float rs = (pf & PF_ACTIVE) ? rf.x + dt * d : 0.f;
       a.rho_star[i] = rs;
       if (is_dyn) {
         const float err = fmaxf(rs - a.rest_density[i], 0.f);
-        kap = fminf((err / (a.dt * a.dt)) * rf.y, a.max_kappa);
+        kap = fminf((err / (dt * dt)) * rf.y, a.max_kappa);
         term += (double)err;
       }
     } else if (is_dyn) {
       const float dc = fmaxf(d, 0.f);
-      kap = fminf((1.0f / a.dt) * dc * rf.x * rf.y, a.max_kappa);
+      kap = fminf((1.0f / dt) * dc * rf.x * rf.y, a.max_kappa);
       term += (double)dc;
     }
     if (a.kappa_new) {
@@ -324,10 +332,13 @@ struct CorrectArgs {
   NbrList L;
   int use_lists;
   const DfsphDev* ctrl;
+  const fs_frame_clock* clock;
 };
 
 __global__ void FS_NB_BOUNDS k_correct(CorrectArgs a) {
   if (a.ctrl && a.ctrl->done) return;
+  if (clock_idle(a.clock)) return;
+  const float dt = a.clock ? a.clock->dt : a.dt;
   for_slots(a.n, [&](int64_t s) {
     const float4 xi = a.xs[s];
     const int32_t i = a.g.perm[s];
@@ -348,9 +359,9 @@ __global__ void FS_NB_BOUNDS k_correct(CorrectArgs a) {
         dvy = fmaf(c, dy, dvy);
         dvz = fmaf(c, dz, dvz);
       });
-      v.x = v.x - a.dt * dvx;
-      v.y = v.y - a.dt * dvy;
-      v.z = v.z - a.dt * dvz;
+      v.x = v.x - dt * dvx;
+      v.y = v.y - dt * dvy;
+      v.z = v.z - dt * dvz;
       a.vstar[s] = v;
     }
     if (a.vstar_api) st3(a.vstar_api, i, xyz(v));
@@ -366,9 +377,11 @@ __global__ void k_kappa_ratio(int64_t n, const float* __restrict__ kappa, const 
 
 // integrate_positions (341-353); also publishes v* in original order.
 __global__ void k_integrate(int64_t n, const int32_t* __restrict__ perm, const float4* __restrict__ xs,
-                            const float4* __restrict__ vstar, float dt, float* x_out, float* vstar_api) {
+                            const float4* __restrict__ vstar, float dt, float* x_out, float* vstar_api,
+                            const fs_frame_clock* clock) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
+  if (s >= n || clock_idle(clock)) return;
+  if (clock) dt = clock->dt;
   const float4 xi = xs[s];
   const float4 v = vstar[s];
   const int32_t i = perm[s];
@@ -381,9 +394,9 @@ __global__ void k_integrate(int64_t n, const int32_t* __restrict__ perm, const f
 // copy v* -> particle_qd then apply_bounds (407-442, unconditional damping)
 __global__ void k_final(int64_t n, const int32_t* __restrict__ perm, const float4* __restrict__ xs,
                         const float4* __restrict__ vstar, Walls walls, float* x_out, float* v_out,
-                        float* vstar_api) {
+                        float* vstar_api, const fs_frame_clock* clock) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
+  if (s >= n || clock_idle(clock)) return;
   const float4 xi = xs[s];
   const float4 v4 = vstar[s];
   const int32_t i = perm[s];
@@ -416,6 +429,7 @@ int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float 
              float* d_rho_dt, float* rho_star, float* kappa_new, float* kratio_new, DfsphDev* ctrl,
              cudaStream_t st, bool use_lists = true) {
   RateArgs a;
+  a.clock = c->clock;
   a.g = grid_view(c);
   a.L = nbr_list(c);
   a.use_lists = use_lists ? 1 : 0;
@@ -449,6 +463,7 @@ int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float 
 int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float* kappa, const float* kratio,
                 float* kappa_api, float* vstar_api, const DfsphDev* ctrl, cudaStream_t st, bool use_lists = true) {
   CorrectArgs a;
+  a.clock = c->clock;
   a.g = grid_view(c);
   a.L = nbr_list(c);
   a.use_lists = use_lists ? 1 : 0;
@@ -472,6 +487,7 @@ int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float
 int run_density_factor(fs_context* c, const fs_model* m, float h, int min_nb, float* rho, float* factor,
                        int32_t* count, cudaStream_t st) {
   DensFactorArgs a;
+  a.clock = c->clock;
   a.g = grid_view(c);
   a.L = nbr_list(c);
   a.n = m->n;
@@ -498,8 +514,70 @@ using namespace fs;
 
 extern "C" {
 
+}  // extern "C"
+
+namespace fs {
+namespace {
+// A clocked substep after its frame is complete: state_out = state_in for
+// every field both states give.
+__global__ void k_idle_copy_dfsph(int64_t n, const fs_frame_clock* clock, fs_state si, fs_state so) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !clock_idle(clock)) return;
+  st3(so.particle_q, i, ld3(si.particle_q, i));
+  st3(so.particle_qd, i, ld3(si.particle_qd, i));
+  if (si.v_star && so.v_star) st3(so.v_star, i, ld3(si.v_star, i));
+  const float* in[] = {si.rho, si.factor, si.rho_star, si.d_rho_dt, si.kappa, si.kappa_v};
+  float* out[] = {so.rho, so.factor, so.rho_star, so.d_rho_dt, so.kappa, so.kappa_v};
+  for (int k = 0; k < 6; ++k)
+    if (in[k] && out[k]) out[k][i] = in[k][i];
+  if (si.neighbor_count && so.neighbor_count) so.neighbor_count[i] = si.neighbor_count[i];
+}
+
+// Sets the context's clock for the span of a clocked substep.
+struct ClockScope {
+  fs_context* c;
+  ClockScope(fs_context* ctx, const fs_frame_clock* clock) : c(ctx) { c->clock = clock; }
+  ~ClockScope() { c->clock = nullptr; }
+};
+}  // namespace
+
+int dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so, const fs_dfsph_params* p,
+                  float* accel, fs_stream_t stream);
+}  // namespace fs
+
+extern "C" {
+
 int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so, const fs_dfsph_params* p,
                      float* accel, fs_stream_t stream) {
+  if (!c) return set_error(FS_ERR_INVALID, "fs_dfsph_substep: null argument");
+  ClockScope cs(c, nullptr);
+  return dfsph_substep(c, m, si, so, p, accel, stream);
+}
+
+int fs_dfsph_substep_clocked(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so,
+                             const fs_dfsph_params* p, float* accel, const fs_frame_clock* clock,
+                             fs_stream_t stream) {
+  if (!c || !clock || !si || !so || !m) return set_error(FS_ERR_INVALID, "fs_dfsph_substep_clocked: null argument");
+  int rc;
+  {
+    ClockScope cs(c, clock);
+    rc = dfsph_substep(c, m, si, so, p, accel, stream);
+  }
+  if (rc || m->n == 0) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  {
+    PassScope ps_(c, P_OTHER, st);
+    k_idle_copy_dfsph<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, clock, *si, *so);
+  }
+  return launch_check("fs_dfsph_substep_clocked");
+}
+
+}  // extern "C"
+
+namespace fs {
+
+int dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state* so, const fs_dfsph_params* p,
+                  float* accel, fs_stream_t stream) {
   if (!c || !m || !si || !so || !p) return set_error(FS_ERR_INVALID, "fs_dfsph_substep: null argument");
   if (m->n < 0) return set_error(FS_ERR_INVALID, "fs_dfsph_substep: negative n");
   if (m->n == 0) return FS_OK;
@@ -521,7 +599,7 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   int rc;
   if ((rc = check_cuda(cudaMemsetAsync(c->dfsph, 0, sizeof(DfsphDev) * 2, st), "dfsph reset"))) return rc;
   // ---- first half: positions x_in
-  if ((rc = grid_build(c, si->particle_q, n, h, st, nullptr))) return rc;
+  if ((rc = grid_build(c, si->particle_q, n, h, st, nullptr, c->clock))) return rc;
   {
     PassScope ps_(c, P_GATHER, st);
     k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, si->particle_q, si->particle_qd, c->xs, c->vs,
@@ -549,6 +627,7 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   aa.dt = dt;
   aa.accel = accel;
   aa.vstar = c->vs2;
+  aa.clock = c->clock;
   {
     PassScope ps_(c, P_DFSPH_ACCEL, st);
     k_accel_predict<<<nb_blocks(c, n), c->nb_block, 0, st>>>(aa);
@@ -570,11 +649,12 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   }
   {
     PassScope ps_(c, P_DFSPH_INTEGRATE, st);
-    k_integrate<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, dt, so->particle_q, so->v_star);
+    k_integrate<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, dt, so->particle_q, so->v_star,
+                                                   c->clock);
   }
   if ((rc = launch_check("dfsph integrate"))) return rc;
   // ---- second half: positions x_out
-  if ((rc = grid_build(c, so->particle_q, n, h, st, nullptr))) return rc;
+  if ((rc = grid_build(c, so->particle_q, n, h, st, nullptr, c->clock))) return rc;
   {
     PassScope ps_(c, P_GATHER, st);
     k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, so->particle_q, so->v_star, c->xs, c->vs2, c->mv,
@@ -599,11 +679,16 @@ int fs_dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_st
   const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 1, 0.f, 0.f);
   {
     PassScope ps_(c, P_DFSPH_FINAL, st);
-    k_final<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, w, so->particle_q, so->particle_qd, so->v_star);
+    k_final<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->xs, c->vs2, w, so->particle_q, so->particle_qd, so->v_star,
+                                              c->clock);
   }
   c->last_stream = st;
   return launch_check("dfsph final");
 }
+
+}  // namespace fs
+
+extern "C" {
 
 int fs_dfsph_info_read(fs_context* c, fs_dfsph_info* info) {
   if (!c || !info) return set_error(FS_ERR_INVALID, "fs_dfsph_info_read: bad arguments");
@@ -662,6 +747,7 @@ int fs_dfsph_nonpressure_predict(fs_context* c, const fs_model* m, const float* 
   aa.dt = dt;
   aa.accel = accel;
   aa.vstar = c->vs2;
+  aa.clock = nullptr;
   k_accel_predict<<<nb_blocks(c, n), c->nb_block, 0, st>>>(aa);
   k_scatter_xyz<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, c->vs2, v_star);
   return launch_check("fs_dfsph_nonpressure_predict");

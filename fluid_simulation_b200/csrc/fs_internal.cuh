@@ -116,6 +116,9 @@ struct fs_context {
   // frame metrics scratch (fs_metrics.cu)
   void* metrics = nullptr;
 
+  // the frame clock of the clocked substep in progress (null otherwise)
+  const fs_frame_clock* clock = nullptr;
+
   // launch tuning of the neighbour kernels (fs_context_set_tuning)
   int32_t nb_block = 128;      // threads per block: 64, 128 or 256
   int32_t nb_ppt = 1;          // particles per thread: 1, 2 or 4

@@ -55,13 +55,14 @@ class FrameGraph:
 
 
 class DeviceFrameLoop:
-    """The WCSPH dam-break frame loop with its substep rule on the device.
+    """The WCSPH / DFSPH dam-break frame loop with its substep rule on the device.
 
-    The reference harness (simulation.py:155-196) reads max |v| and max |a|
-    back to the host before every substep to choose its dt.  Here a frame
-    clock in device memory carries the time left in the frame; one CUDA graph
-    records ``graph_substeps`` pairs of [evaluate the rule on the device
-    (fs_frame_clock_advance), clocked substep (fs_wcsph_substep_clocked)],
+    The reference harness (simulation.py:155-196) reads max |v| (and for
+    WCSPH max |a|) back to the host before every substep to choose its dt.
+    Here a frame clock in device memory carries the time left in the frame;
+    one CUDA graph records ``graph_substeps`` pairs of [evaluate the rule on
+    the device (fs_frame_clock_advance), clocked substep
+    (fs_wcsph_substep_clocked / fs_dfsph_substep_clocked)],
     and a frame replays that graph until the clock reports the frame done:
     one read of the clock per replay instead of one per substep.  Substeps
     after the end of the frame copy their input through, so the result is
@@ -72,8 +73,8 @@ class DeviceFrameLoop:
     MAX_SUBSTEPS = 4096  # the harness's own limit per frame
 
     def __init__(self, sim, graph_substeps: int = 64):
-        if sim.method != "wcsph":
-            raise NotImplementedError("the device-side substep rule drives the WCSPH solver")
+        if sim.method not in ("wcsph", "dfsph"):
+            raise NotImplementedError("the device-side substep rule drives the CFL solvers (WCSPH, DFSPH)")
         if graph_substeps < 2 or graph_substeps % 2:
             raise ValueError("graph_substeps must be even and >= 2")
         from .solver import _common as cm
@@ -88,12 +89,16 @@ class DeviceFrameLoop:
         start.run_substeps = 1 if sim.total_substeps else 0
         self.clock.copy_(torch.frombuffer(bytearray(bytes(start)), dtype=torch.uint8))
         mat = sim.material
-        self.rule = _lib.CflRule(sim.frame_dt, sim.frame_dt / sim.substeps, 0, 1, float(solver.smoothing_length),
-                                 math.sqrt(mat["stiffness"] * mat["exponent"] / sim.scene.spec.density),
-                                 float(mat["viscosity"]), float(sim.scene.spacing))
-        self._ms = cm.model_struct(model, wcsph=True)
+        wcsph = sim.method == "wcsph"
+        sound = math.sqrt(mat["stiffness"] * mat["exponent"] / sim.scene.spec.density) if wcsph else 0.0
+        self.rule = _lib.CflRule(sim.frame_dt, sim.frame_dt / sim.substeps, 0 if wcsph else 1, 1 if wcsph else 0,
+                                 float(solver.smoothing_length), sound, float(mat["viscosity"]),
+                                 float(sim.scene.spacing))
+        self._ms = cm.model_struct(model, wcsph=wcsph)
         a, b = sim.state_0, sim.state_1
-        self._si = [cm.state_struct(s, n, dev, need=("rho", "pressure")) for s in (a, b)]
+        need = ("rho", "pressure") if wcsph else tuple(vars(a.sph))
+        self._si = [cm.state_struct(s, n, dev, need=need) for s in (a, b)]
+        lib_fn = "fs_wcsph_substep_clocked" if wcsph else "fs_dfsph_substep_clocked"
         self._v = [s.particle_qd for s in (a, b)]
         self._params = solver.params(0.0)
         self._acc = solver._particle_accel
@@ -109,9 +114,9 @@ class DeviceFrameLoop:
                 i, o = k % 2, 1 - k % 2
                 _lib.check(lib.fs_frame_clock_advance(ck, C.byref(self.rule), self._v[i].data_ptr(), n,
                                                       self._acc.data_ptr(), n, st), "clock advance")
-                _lib.check(lib.fs_wcsph_substep_clocked(self._ctx, C.byref(self._ms), C.byref(self._si[i]),
-                                                        C.byref(self._si[o]), C.byref(self._params),
-                                                        self._acc.data_ptr(), ck, st), "clocked substep")
+                _lib.check(getattr(lib, lib_fn)(self._ctx, C.byref(self._ms), C.byref(self._si[i]),
+                                                C.byref(self._si[o]), C.byref(self._params), self._acc.data_ptr(),
+                                                ck, st), "clocked substep")
         torch.cuda.current_stream(dev).wait_stream(self.stream)
         self.replays = 0
 

@@ -337,6 +337,11 @@ int fs_frame_clock_advance(fs_frame_clock* clock, const fs_cfl_rule* rule, const
 int fs_wcsph_substep_clocked(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
                              const fs_wcsph_params* params, float* accel, const fs_frame_clock* clock,
                              fs_stream_t stream);
+/* fs_dfsph_substep at dt = clock->dt (rule method 1); once the frame is
+ * complete it copies state_in to state_out (every field both give). */
+int fs_dfsph_substep_clocked(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
+                             const fs_dfsph_params* params, float* accel, const fs_frame_clock* clock,
+                             fs_stream_t stream);
 
 /* Frame metrics of the dam-break harness (simulation.py:198-225) reduced on
  * the device into out[14] (device doubles): [0] non-finite x or v, [1]

@@ -44,27 +44,36 @@ def test_frame_graph_matches_plain_launches(kind, cls, dt, cuda_device):
     assert torch.equal(out.sph.rho, a.sph.rho)
 
 
-def test_device_frame_loop_equals_host_loop(cuda_device):
-    """Two WCSPH dam-break frames with the substep rule evaluated on the
-    device (one graph of 16 clocked substeps, replayed until the frame is
-    done) end in the same bits, after the same number of substeps, as the
-    reference harness loop that reads the maxima back before every substep."""
+@pytest.mark.parametrize("method,graph_substeps,frames", [("wcsph", 16, 2), ("dfsph", 2, 3)])
+def test_device_frame_loop_equals_host_loop(method, graph_substeps, frames, cuda_device):
+    """Dam-break frames with the substep rule evaluated on the device (one
+    graph of clocked substeps, replayed until the frame is done) end in the
+    same bits, after the same number of substeps, as the reference harness
+    loop that reads the maxima back before every substep.  DFSPH starts at
+    4 m/s, so that its speed limit (0.4 spacing / |v|) cuts its substeps
+    below 1/240 s."""
     from fluid_simulation_b200.dam_break import DamBreakSimulation
     from fluid_simulation_b200.graph import DeviceFrameLoop
 
     s = make_scene(10000)
-    host = DamBreakSimulation(s, "wcsph", device=cuda_device)
-    dev = DamBreakSimulation(s, "wcsph", device=cuda_device)
-    loop = DeviceFrameLoop(dev, graph_substeps=16)
-    for _ in range(2):
+    host = DamBreakSimulation(s, method, device=cuda_device)
+    dev = DamBreakSimulation(s, method, device=cuda_device)
+    if method == "dfsph":
+        for sim in (host, dev):
+            sim.state_0.particle_qd[:, 0] = 4.0
+    loop = DeviceFrameLoop(dev, graph_substeps=graph_substeps)
+    counts = []
+    for _ in range(frames):
         host.step()
         loop.step()
         torch.cuda.synchronize()
-        assert dev.last_substeps == host.last_substeps > 16  # several replays per frame
+        assert dev.last_substeps == host.last_substeps
+        counts.append(host.last_substeps)
+    assert max(counts) > graph_substeps  # several replays per frame
     assert torch.equal(dev.state_0.particle_q, host.state_0.particle_q)
     assert torch.equal(dev.state_0.particle_qd, host.state_0.particle_qd)
     assert torch.equal(dev.state_0.sph.rho, host.state_0.sph.rho)
-    assert dev.total_substeps == host.total_substeps and loop.replays >= 2 * 2
+    assert dev.total_substeps == host.total_substeps
 
 
 def test_device_frame_loop_reports_nonfinite_state(cuda_device):
