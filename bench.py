@@ -417,7 +417,7 @@ def time_frame_loop(dev, flush, target=400000, frames=2, method="wcsph"):
     s = make_scene(target)
     host = DamBreakSimulation(s, method, device=dev)
     devs = DamBreakSimulation(s, method, device=dev)
-    loop = DeviceFrameLoop(devs, graph_substeps=64 if method == "wcsph" else 8)
+    loop = DeviceFrameLoop(devs, graph_substeps=64 if method == "wcsph" else devs.substeps)
     host.step()
     loop.step()  # first frame: warm-up of both
     torch.cuda.synchronize()
