@@ -186,7 +186,7 @@ struct RateArgs {
   float* d_rho_dt;          // API
   float* rho_star;          // API (mode 0)
   float* kappa_new;         // cell order candidate kappa
-  float* kratio_new;        // cell order kappa / max(rho, 1e-6) (the correction's per-particle term)
+  float2* kratio_new;       // cell order (kappa / max(rho, 1e-6), mass): what the correction gathers per neighbour
   NbrList L;
   int use_lists;
   DfsphDev* ctrl;           // null: separate-pass use, no residual
@@ -309,7 +309,7 @@ __global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
     }
     if (a.kappa_new) {
       a.kappa_new[s] = kap;
-      a.kratio_new[s] = kap / fmaxf(rf.x, 1.0e-6f);
+      a.kratio_new[s] = make_float2(kap / fmaxf(rf.x, 1.0e-6f), a.vstar[s].w);
     }
     dyn += is_dyn ? 1 : 0;
   });
@@ -325,7 +325,7 @@ struct CorrectArgs {
   const float4* xs;
   float4* vstar;          // in/out (own slot only)
   const float* kappa;     // cell order (committed to the API array)
-  const float* kratio;    // cell order kappa / max(rho, 1e-6)
+  const float2* kratio;   // cell order (kappa / max(rho, 1e-6), mass): one gather per neighbour
   float h, dt;
   float* kappa_api;       // commit kappa to the API array (may be null)
   float* vstar_api;       // optional original-order v* output
@@ -346,7 +346,7 @@ __global__ void FS_NB_BOUNDS k_correct(CorrectArgs a) {
     float4 v = a.vstar[s];
     if (pf_of(xi) & PF_DYNAMIC) {
       const Cubic K(a.h);
-      const float ci = a.kratio[s];
+      const float ci = a.kratio[s].x;
       float dvx = 0.f, dvy = 0.f, dvz = 0.f;
       const bool lists_ok = a.use_lists && lists_usable(a.L);
       visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
@@ -354,7 +354,8 @@ __global__ void FS_NB_BOUNDS k_correct(CorrectArgs a) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         float r, rinv;
         r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-        const float c = __ldg(&a.vstar[t].w) * (ci + __ldg(a.kratio + t)) * K.grad_scale(r, rinv);
+        const float2 kj = __ldg(a.kratio + t);
+        const float c = kj.y * (ci + kj.x) * K.grad_scale(r, rinv);
         dvx = fmaf(c, dx, dvx);
         dvy = fmaf(c, dy, dvy);
         dvz = fmaf(c, dz, dvz);
@@ -370,9 +371,9 @@ __global__ void FS_NB_BOUNDS k_correct(CorrectArgs a) {
 
 // kappa / max(rho, 1e-6) of gathered kappas (warm start, separate pass)
 __global__ void k_kappa_ratio(int64_t n, const float* __restrict__ kappa, const float2* __restrict__ sc2,
-                              float* __restrict__ kratio) {
+                              const float4* __restrict__ vm, float2* __restrict__ kratio) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n) kratio[s] = kappa[s] / fmaxf(sc2[s].x, 1.0e-6f);
+  if (s < n) kratio[s] = make_float2(kappa[s] / fmaxf(sc2[s].x, 1.0e-6f), vm[s].w);
 }
 
 // integrate_positions (341-353); also publishes v* in original order.
@@ -426,7 +427,7 @@ __global__ void k_residual(int64_t n, const int32_t* __restrict__ flags, const i
 }
 
 int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float dt, float max_kappa, float eta,
-             float* d_rho_dt, float* rho_star, float* kappa_new, float* kratio_new, DfsphDev* ctrl,
+             float* d_rho_dt, float* rho_star, float* kappa_new, float2* kratio_new, DfsphDev* ctrl,
              cudaStream_t st, bool use_lists = true) {
   RateArgs a;
   a.clock = c->clock;
@@ -460,7 +461,7 @@ int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float 
   return launch_check("dfsph rate");
 }
 
-int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float* kappa, const float* kratio,
+int run_correct(fs_context* c, const fs_model* m, float h, float dt, const float* kappa, const float2* kratio,
                 float* kappa_api, float* vstar_api, const DfsphDev* ctrl, cudaStream_t st, bool use_lists = true) {
   CorrectArgs a;
   a.clock = c->clock;
@@ -637,15 +638,15 @@ int dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state
     {
       PassScope ps_(c, P_GATHER, st, 2);
       k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa, c->sc1, nullptr);
-      k_kappa_ratio<<<blocks_for(n), kBlock, 0, st>>>(n, c->sc1, c->sc2, c->sc1b);
+      k_kappa_ratio<<<blocks_for(n), kBlock, 0, st>>>(n, c->sc1, c->sc2, c->vs2, c->krm);
     }
-    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa, nullptr, nullptr, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->krm, so->kappa, nullptr, nullptr, st))) return rc;
   }
   for (int it = 0; it < p->max_rho_iterations; ++it) {
     if ((rc = run_rate(c, m, 0, it, h, dt, p->max_kappa, p->eta_density, so->d_rho_dt, so->rho_star, c->sc1,
-                       c->sc1b, c->dfsph + 0, st)))
+                       c->krm, c->dfsph + 0, st)))
       return rc;
-    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa, nullptr, c->dfsph + 0, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->krm, so->kappa, nullptr, c->dfsph + 0, st))) return rc;
   }
   {
     PassScope ps_(c, P_DFSPH_INTEGRATE, st);
@@ -666,15 +667,15 @@ int dfsph_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_state
     {
       PassScope ps_(c, P_GATHER, st, 2);
       k_gather_scalar<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, si->kappa_v, c->sc1, nullptr);
-      k_kappa_ratio<<<blocks_for(n), kBlock, 0, st>>>(n, c->sc1, c->sc2, c->sc1b);
+      k_kappa_ratio<<<blocks_for(n), kBlock, 0, st>>>(n, c->sc1, c->sc2, c->vs2, c->krm);
     }
-    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa_v, nullptr, nullptr, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->krm, so->kappa_v, nullptr, nullptr, st))) return rc;
   }
   for (int it = 0; it < p->max_vel_iterations; ++it) {
     if ((rc = run_rate(c, m, 1, it, h, dt, p->max_kappa_v, p->eta_divergence, so->d_rho_dt, nullptr, c->sc1,
-                       c->sc1b, c->dfsph + 1, st)))
+                       c->krm, c->dfsph + 1, st)))
       return rc;
-    if ((rc = run_correct(c, m, h, dt, c->sc1, c->sc1b, so->kappa_v, nullptr, c->dfsph + 1, st))) return rc;
+    if ((rc = run_correct(c, m, h, dt, c->sc1, c->krm, so->kappa_v, nullptr, c->dfsph + 1, st))) return rc;
   }
   const Walls w = make_walls(p->bound_width, p->bound_height, p->bound_length, p->boundary_damping, 1, 0.f, 0.f);
   {
@@ -780,9 +781,9 @@ int fs_dfsph_correct(fs_context* c, const fs_model* m, const float* x, float* v_
   k_gather_scalar<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, kappa, c->sc1, nullptr);
   {
     PassScope ps_(c, P_GATHER, st);
-    k_kappa_ratio<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->sc1, c->sc2, c->sc1b);
+    k_kappa_ratio<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->sc1, c->sc2, c->vs2, c->krm);
   }
-  return run_correct(c, m, h, dt, c->sc1, c->sc1b, nullptr, v_star, nullptr, st, false);
+  return run_correct(c, m, h, dt, c->sc1, c->krm, nullptr, v_star, nullptr, st, false);
 }
 
 int fs_dfsph_residual(fs_context* c, const fs_model* m, const float* a, const float* b, double* out,

@@ -427,6 +427,7 @@ static int context_alloc(fs_context* c, int64_t capacity, int64_t ncell) {
       {(void**)&c->vs, sizeof(float4) * cap},           {(void**)&c->vs2, sizeof(float4) * cap},
       {(void**)&c->mv, sizeof(float) * cap},            {(void**)&c->sc2, sizeof(float2) * cap},
       {(void**)&c->sc1, sizeof(float) * cap},           {(void**)&c->sc1b, sizeof(float) * cap},
+      {(void**)&c->krm, sizeof(float2) * cap},
       {(void**)&c->xo_tmp, sizeof(float) * 3 * cap},    {(void**)&c->vo_tmp, sizeof(float) * 3 * cap},
       {(void**)&c->red_part, sizeof(double) * rb},      {(void**)&c->red_cnt, sizeof(int64_t) * rb},
       {(void**)&c->dfsph, sizeof(DfsphDev) * 2},         {(void**)&c->status, sizeof(uint32_t)},
@@ -461,7 +462,7 @@ int fs_context_destroy(fs_context* c) {
   DeviceGuard dg(c->device);
   timer_free(c->timer);
   void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
-                c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
+                c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->krm, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
                 c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds, c->metrics};
   for (void* p : ps)
     if (p) cudaFree(p);
