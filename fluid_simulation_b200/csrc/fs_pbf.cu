@@ -164,7 +164,7 @@ struct LambdaArgs {
   const float* rest_density;
   float h, eps;
   int min_nb;
-  float* lam_s;       // cell order
+  float2* lam_s;      // cell order (lambda, mass): what the delta pass gathers per neighbour
   float* lam;         // API
   float* rho;         // API
   int32_t* count;     // API
@@ -177,7 +177,7 @@ __global__ void FS_NB_BOUNDS_PBF k_lambda(LambdaArgs a) {
     const int32_t i = a.g.perm[s];
     if (!(pf_of(xi) & PF_DYNAMIC)) {
       a.L.cnt[s] = 0;
-      a.lam_s[s] = 0.f;
+      a.lam_s[s] = make_float2(0.f, a.vs[s].w);
       if (a.lam) a.lam[i] = 0.f;
       if (a.rho) a.rho[i] = 0.f;
       if (a.count) a.count[i] = 0;
@@ -209,7 +209,7 @@ __global__ void FS_NB_BOUNDS_PBF k_lambda(LambdaArgs a) {
     sq = fmaf(gx, gx, fmaf(gy, gy, fmaf(gz, gz, sq)));
     const float ci = fmaxf(rho / rho0 - 1.0f, 0.f);
     const float l = (a.min_nb > 0 && cnt < a.min_nb) ? 0.f : -ci / (sq + a.eps);
-    a.lam_s[s] = l;
+    a.lam_s[s] = make_float2(l, a.vs[s].w);
     if (a.lam) a.lam[i] = l;
     if (a.rho) a.rho[i] = rho;
     if (a.count) a.count[i] = cnt;
@@ -225,7 +225,7 @@ struct DeltaArgs {
   int64_t n;
   const float4* xs;
   const float4* vs;   // .w = mass
-  const float* lam_s;
+  const float2* lam_s;  // (lambda, mass), one gather per neighbour
   const float* rest_density;
   float h, scorr_k, scorr_n, w_dq, max_dp;
   int clamp;
@@ -244,7 +244,7 @@ __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
       return;
     }
     const float rho0 = fmaxf(a.rest_density[i], 1.0e-6f);
-    const float li = a.lam_s[s];
+    const float li = a.lam_s[s].x;
     const Poly6Spiky K(a.h);
     const bool scorr = a.scorr_k != 0.f && !(a.w_dq <= 1.0e-6f);
     const float inv_wdq = scorr ? 1.0f / a.w_dq : 0.f;
@@ -258,7 +258,8 @@ __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
       r_and_inv(r2, r, rinv);
       float sc = 0.f;
       if (scorr) sc = -a.scorr_k * powf(K.w_r2(r2) * inv_wdq, a.scorr_n);
-      const float c = (li + __ldg(a.lam_s + t) + sc) * __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
+      const float2 lj = __ldg(a.lam_s + t);
+      const float c = (li + lj.x + sc) * lj.y * K.grad_scale(r, rinv);
       dx_ = fmaf(c, dx, dx_);
       dy_ = fmaf(c, dy, dy_);
       dz_ = fmaf(c, dz, dz_);
@@ -282,7 +283,8 @@ __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
 
 // update_velocity_from_positions (403-416), cell order; .w keeps the mass
 __global__ void k_velocity(int64_t n, const float4* __restrict__ xs, const float4* __restrict__ xin,
-                           const float4* __restrict__ vs, float dt, float4* __restrict__ vout) {
+                           const float4* __restrict__ vs, const float2* __restrict__ sc2, float dt,
+                           float4* __restrict__ vout) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const float4 xi = xs[s];
@@ -293,7 +295,7 @@ __global__ void k_velocity(int64_t n, const float4* __restrict__ xs, const float
     const float d = fmaxf(dt, 1.0e-8f);
     v = make_float3((xi.x - x0.x) / d, (xi.y - x0.y) / d, (xi.z - x0.z) / d);
   }
-  vout[s] = make_float4(v.x, v.y, v.z, vi.w);
+  vout[s] = make_float4(v.x, v.y, v.z, sc2[s].y);  // .w: m / max(rho, 1e-6), XSPH's neighbour weight
 }
 
 // apply_xsph_viscosity (435-463) + copy x_pred -> particle_q + apply_bounds (467-517)
@@ -303,7 +305,7 @@ struct XsphArgs {
   int use_lists;
   int64_t n;
   const float4* xs;
-  const float4* vel;   // (v, mass) cell order
+  const float4* vel;   // (v, m / max(rho, 1e-6)) cell order
   const float2* sc2;   // rho
   float h, c;
   Walls walls;
@@ -329,9 +331,9 @@ __global__ void FS_NB_BOUNDS_PBF k_xsph_final(XsphArgs a) {
         visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
                             [&](int t, float4 xj) {
           const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-          const float4 vj = __ldg(a.vel + t);
+          const float4 vj = __ldg(a.vel + t);  // (v, m / max(rho, 1e-6))
           // (m_j / max(rho_j, 1e-6)) W(r), the ratio from the final density pass
-          const float w = __ldg(&a.sc2[t].y) * K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+          const float w = vj.w * K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
           cx = fmaf(vj.x - vi.x, w, cx);
           cy = fmaf(vj.y - vi.y, w, cy);
           cz = fmaf(vj.z - vi.z, w, cz);
@@ -358,11 +360,22 @@ __global__ void k_gather_lambda(int64_t n, const int32_t* __restrict__ perm, con
   if (s < n) out[s] = a[perm[s]];
 }
 
-// (rho, mass / max(rho, 1e-6)) from a cell-order density and the mass in vel.w
-__global__ void k_rho_ratio(int64_t n, const float* __restrict__ rho, const float4* __restrict__ vel,
+// (rho, mass / max(rho, 1e-6)) from a cell-order density and the mass in
+// vel.w; vel.w then holds the ratio (XSPH's neighbour weight)
+__global__ void k_rho_ratio(int64_t n, const float* __restrict__ rho, float4* __restrict__ vel,
                             float2* __restrict__ out) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n) out[s] = make_float2(rho[s], vel[s].w / fmaxf(rho[s], 1.0e-6f));
+  if (s >= n) return;
+  const float ratio = vel[s].w / fmaxf(rho[s], 1.0e-6f);
+  out[s] = make_float2(rho[s], ratio);
+  vel[s].w = ratio;
+}
+
+// (lambda[i], mass) of original order into cell order (mass from the gathered vs.w)
+__global__ void k_gather_lambda_mass(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ lam,
+                                     const float4* __restrict__ vs, float2* __restrict__ out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) out[s] = make_float2(lam[perm[s]], vs[s].w);
 }
 
 int gather_pbf(fs_context* c, const fs_model* m, const float* x_in, cudaStream_t st) {
@@ -455,7 +468,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     la.h = h;
     la.eps = p->lambda_epsilon;
     la.min_nb = p->min_neighbors_for_lambda;
-    la.lam_s = c->sc1;
+    la.lam_s = c->krm;
     la.lam = so->pbf_lambda;
     la.rho = so->rho;
     la.count = so->neighbor_count;
@@ -470,7 +483,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
     da.n = n;
     da.xs = cur;
     da.vs = c->vs;
-    da.lam_s = c->sc1;
+    da.lam_s = c->krm;
     da.rest_density = m->rest_density;
     da.h = h;
     da.scorr_k = p->scorr_k;
@@ -509,7 +522,7 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   }
   {
     PassScope ps_(c, P_PBF_VELOCITY, st);
-    k_velocity<<<blocks_for(n), kBlock, 0, st>>>(n, cur, c->vs2, c->vs, dt, nxt);
+    k_velocity<<<blocks_for(n), kBlock, 0, st>>>(n, cur, c->vs2, c->vs, c->sc2, dt, nxt);
   }
   XsphArgs xa;
   xa.g = gf;
@@ -581,7 +594,7 @@ int fs_pbf_lambda(fs_context* c, const fs_model* m, const float* x_pred, const f
   la.h = p->smoothing_length;
   la.eps = p->lambda_epsilon;
   la.min_nb = p->min_neighbors_for_lambda;
-  la.lam_s = c->sc1;
+  la.lam_s = c->krm;
   la.lam = pbf_lambda;
   la.rho = rho;
   la.count = neighbor_count;
@@ -599,7 +612,7 @@ int fs_pbf_delta(fs_context* c, const fs_model* m, const float* x_pred, const fl
   cudaStream_t st = (cudaStream_t)stream;
   k_gather_common<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, *m, x_pred, x_pred, c->xs, c->vs, nullptr,
                                                        c->status, c->nworlds);
-  k_gather_lambda<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, pbf_lambda, c->sc1);
+  k_gather_lambda_mass<<<blocks_for(m->n), kBlock, 0, st>>>(m->n, c->perm, pbf_lambda, c->vs, c->krm);
   DeltaArgs da;
   da.g = grid_view(c);
   da.L = nbr_list(c);
@@ -607,7 +620,7 @@ int fs_pbf_delta(fs_context* c, const fs_model* m, const float* x_pred, const fl
   da.n = m->n;
   da.xs = c->xs;
   da.vs = c->vs;
-  da.lam_s = c->sc1;
+  da.lam_s = c->krm;
   da.rest_density = m->rest_density;
   da.h = p->smoothing_length;
   da.scorr_k = p->scorr_k;
