@@ -199,12 +199,19 @@ def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1):
 # ------------------------------------------------------ batched scenes ----
 def batched_configs(batch, kind):
     """Solver config and dt of a batch of dam-break scenes: the reference
-    harness's PBF config (4 iterations, ...) at dt = 1/240, or WCSPH at the
-    acoustic limit 0.25 h / c0 of the stiffest scene.  Walls come from each
-    scene (the config's bound_* apply only to the plain per-scene runs)."""
-    from fluid_simulation_b200.solver import SolverPBF, SolverWCSPH
+    harness's PBF config (4 iterations, ...) at dt = 1/240, its DFSPH config
+    (5 density / 12 divergence iterations, no warm start) at the harness's
+    1/240 cap (the columns start at rest, and after the timed frames they
+    fall at under 1 m/s, below the 0.4 spacing / max|v| limit), or WCSPH at
+    the acoustic limit 0.25 h / c0 of the stiffest scene.  Walls come from
+    each scene (the config's bound_* apply only to the plain per-scene runs)."""
+    from fluid_simulation_b200.solver import SolverDFSPH, SolverPBF, SolverWCSPH
     common = dict(particle_radius=batch.radius, particle_length=batch.spacing, smoothing_length_coff=2.0,
                   boundary_damping=0.0)
+    if kind == "dfsph":
+        return SolverDFSPH, (lambda walls: SolverDFSPH.SphConfig(
+            max_rho_iterations=5, max_vel_iterations=12, warm_start=False, max_kappa=1.0, max_kappa_v=100.0,
+            bound_width=walls[0], bound_height=walls[1], bound_length=walls[2], **common)), 1.0 / 240.0, 4
     if kind == "pbf":
         return SolverPBF, (lambda walls: SolverPBF.PbfConfig(
             max_iterations=4, lambda_epsilon=100.0, min_neighbors_for_lambda=8, scorr_k=0.0,
@@ -286,6 +293,17 @@ def time_batched(kind, dev, flush, frames=2, warm=1):
     xb = fb.result.particle_q
     same = all(torch.equal(xb[int(b.starts[k]):int(b.starts[k + 1])], g.result.particle_q)
                for k, g in enumerate(graphs))
+    extra = {}
+    if kind == "dfsph":  # per-world decisions: each scene's iteration counts as it took them alone
+        per_world = sb.last_world_iterations()
+        alone = [sv.last_iterations() for m, sv, a, c in scenes]
+        key = lambda d: (d["rho_iterations"], d["vel_iterations"])
+        extra = dict(iterations_equal_to_serial=all(key(p) == key(q) for p, q in zip(per_world, alone)),
+                     last_substep_iterations=dict(
+                         rho=dict(min=min(p["rho_iterations"] for p in per_world),
+                                  max=max(p["rho_iterations"] for p in per_world)),
+                         vel=dict(min=min(p["vel_iterations"] for p in per_world),
+                                  max=max(p["vel_iterations"] for p in per_world))))
     rate = lambda ms: round(n * sub * frames / (ms * 1e-3), 1)
     rec = dict(workload=f"batched_{kind}_256", solver=kind.upper(), scenes=len(b.scenes), particles=n,
                scene_counts="log-uniform [2000, 100000], seed 3; column fraction U(0.2, 0.6); stiffness and "
@@ -297,7 +315,7 @@ def time_batched(kind, dev, flush, frames=2, warm=1):
                serial_graph=dict(value=rate(t_serial_g), ms_per_frame=round(t_serial_g / frames, 3)),
                speedup_vs_serial_eager=round(t_serial / t_batched, 2),
                speedup_vs_serial_graph=round(t_serial_g / t_batched, 2),
-               final_state_bit_identical_to_serial=bool(same), tuning_batched=tuning)
+               final_state_bit_identical_to_serial=bool(same), tuning_batched=tuning, **extra)
     del fb, graphs, scenes, mb, sb
     torch.cuda.empty_cache()
     return rec
@@ -678,7 +696,7 @@ def run_ours(args):
             torch.cuda.empty_cache()
 
     if world == 1 and not args.no_secondary and not args.no_batched:
-        for kind in ("pbf", "wcsph"):
+        for kind in ("pbf", "wcsph", "dfsph"):
             secondary[f"batched_{kind}_256"] = time_batched(kind, dev, flush)
     if world == 1 and not args.no_secondary:
         secondary["wcsph_dam_frames_401856"] = time_frame_loop(dev, flush)
@@ -765,7 +783,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "frames"],
+    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "batched_dfsph", "frames"],
                     help="run one secondary workload alone (profiling); no bench line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -123,6 +123,7 @@ SIGNATURES = {
     "fs_dfsph_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
                                    C.POINTER(DfsphParams), P, P]),
     "fs_dfsph_info_read": (C.c_int, [P, C.POINTER(DfsphInfo)]),
+    "fs_dfsph_info_worlds": (C.c_int, [P, C.POINTER(DfsphInfo), C.c_int32]),
     "fs_pbf_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
                                  C.POINTER(PbfParams), P, P, P]),
     "fs_wcsph_density": (C.c_int, [P, C.POINTER(Model), P, F, I32, P, P, P]),

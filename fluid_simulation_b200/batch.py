@@ -83,16 +83,25 @@ class Batch:
     def per_particle(self, name: str) -> np.ndarray:
         return np.repeat(np.array([getattr(s, name) for s in self.scenes], np.float32), self.counts)
 
-    def boxes(self, h: float | None = None):
+    def boxes(self, h: float | None = None, margin: int = 1):
         """WorldGrid boxes: the cells int(x / h) (truncating, float32 as the
-        device computes them) that the tank of each scene spans."""
+        device computes them) that the tank of each scene spans, widened by
+        ``margin`` cells on every side.  The margin holds particles that a
+        substep carries past a wall before the walls act: DFSPH builds its
+        second grid from positions integrated with v* and clamps them only
+        at the end of the substep, so a particle can lie up to |v*| dt
+        outside its tank there (the harness's substep rule keeps that under
+        0.4 spacing = 0.2 h).  With every particle inside its box, each
+        world's cells, their contents and order equal those of the plain
+        hash grid of that scene alone (the grid clamps a particle beyond the
+        box into the edge cell, which changes DFSPH's candidate counts)."""
         h = self.h if h is None else h
         inv = np.float32(1.0) / np.float32(h)
         out = []
         for s in self.scenes:
             w, hh, l = s.walls
-            lo = [int(np.float32(v) * inv) for v in (-w, -hh, 0.0)]
-            hi = [int(np.float32(v) * inv) for v in (w, hh, 2.0 * l)]
+            lo = [int(np.float32(v) * inv) - margin for v in (-w, -hh, 0.0)]
+            hi = [int(np.float32(v) * inv) + margin for v in (w, hh, 2.0 * l)]
             out.append((tuple(lo), tuple(b - a + 1 for a, b in zip(lo, hi)), s.walls))
         return out
 

@@ -368,6 +368,12 @@ int fs_context_create_worlds(fs_context** out, int64_t capacity, const fs_world_
   if (!rc)
     rc = check_cuda(cudaMemcpy(c->worlds, host, sizeof(WorldDev) * nworlds, cudaMemcpyHostToDevice),
                     "fs_context_create_worlds: copy");
+  if (!rc)
+    rc = check_cuda(cudaMalloc((void**)&c->dfsph_worlds, sizeof(DfsphWorld) * 2 * nworlds),
+                    "fs_context_create_worlds: decisions");
+  if (!rc)
+    rc = check_cuda(cudaMemset(c->dfsph_worlds, 0, sizeof(DfsphWorld) * 2 * nworlds),
+                    "fs_context_create_worlds: memset");
   delete[] host;
   if (rc) {
     fs_context_destroy(c);
@@ -463,7 +469,8 @@ int fs_context_destroy(fs_context* c) {
   timer_free(c->timer);
   void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
                 c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->krm, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
-                c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds, c->metrics};
+                c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds, c->metrics,
+                c->dfsph_worlds};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete c;

@@ -24,8 +24,14 @@ struct DfsphDev {     // device-resident per-step DFSPH control block
   int32_t done;       // residual test passed: later kernels of this half exit
   int32_t iters;      // iterations entered in this half
   uint32_t ticket;    // last-block-done counter of the residual reduction
-  int32_t pad;
+  int32_t worlds_done;  // batched contexts: worlds whose residual test passed (all: done = 1)
   double residual;    // last residual of this half
+};
+
+struct DfsphWorld {   // batched contexts: one world's decisions in one half of the substep
+  int32_t done;       // this world's residual test passed: its particles leave the iterations
+  int32_t iters;      // iterations this world entered
+  double residual;    // its last residual (mean over its dynamic particles)
 };
 
 // Passes for the per-pass CUDA-event timer (fs_timer_*) and launch counter.
@@ -101,6 +107,7 @@ struct fs_context {
   double* red_part = nullptr;   // [reduction blocks]
   int64_t* red_cnt = nullptr;   // [reduction blocks]
   fs::DfsphDev* dfsph = nullptr; // [2] control blocks (density half, divergence half)
+  fs::DfsphWorld* dfsph_worlds = nullptr;  // batched contexts: [2][nworlds] per-world decisions
   uint32_t* status = nullptr;
   unsigned long long* tile_stats = nullptr;  // [2] visits served by lists / by rescans
 

@@ -354,14 +354,20 @@ class HashGrid:
 class WorldGrid(HashGrid):
     """Segmented grid of a batched model: one box of cells per world
     (``Model.particle_world``), keyed (world, cell), and one tank of walls
-    per world.  Drop it in as ``model.particle_grid`` and the WCSPH / PBF
-    solvers advance every world in one launch per pass; the walls of each
-    world replace the solver config's ``bound_*``.
+    per world.  Drop it in as ``model.particle_grid`` and the WCSPH, DFSPH
+    and PBF solvers advance every world in one launch per pass; the walls of
+    each world replace the solver config's ``bound_*``, and DFSPH takes its
+    iteration decisions per world.
 
     ``boxes``: one ``(cell_lo[3], dims[3], (bound_width, bound_height,
     bound_length))`` per world: the box covers the cells whose coordinate
     ``int(x / h)`` (truncating, as the reference's hash grid) lies in
-    ``[cell_lo, cell_lo + dims)``, h = the solver's smoothing length."""
+    ``[cell_lo, cell_lo + dims)``, h = the solver's smoothing length.  A
+    particle outside its box is binned into the nearest edge cell: clamping
+    keeps adjacent cells adjacent, so every neighbour within h is still
+    found, but that cell's contents and order (and DFSPH's candidate counts)
+    differ from the scene's own hash grid (``Batch.boxes`` adds a margin
+    for that)."""
 
     def __init__(self, boxes, device="cuda:0"):
         super().__init__(1, 1, 1, device=device, rounding=1)

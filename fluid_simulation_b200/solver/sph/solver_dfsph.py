@@ -5,7 +5,9 @@ the reference ``SolverDFSPH``.  The reference reads each solver iteration's
 residual back to the host (solver_dfsph.py:733, 849); here the residual and
 the break test run on the device (``fs_dfsph_substep``), so a step issues no
 host synchronisation and takes the same iteration decisions.
-``last_iterations()`` reads the decisions back on demand.
+``last_iterations()`` reads the decisions back on demand.  On a batched model
+(``newton_shim.WorldGrid``) each world takes its own decisions, as its scene
+would alone; ``last_world_iterations()`` reads them per world.
 """
 
 from __future__ import annotations
@@ -96,6 +98,19 @@ class SolverDFSPH(SolverBase):
                    "SolverDFSPH.last_iterations")
         return dict(rho_iterations=info.rho_iterations, vel_iterations=info.vel_iterations,
                     density_residual=info.density_residual, divergence_residual=info.divergence_residual)
+
+    def last_world_iterations(self) -> list:
+        """Per-world iteration counts and residuals of the last step of a
+        batched model (synchronises); one dict per world."""
+        ctx = cm.grid_ctx(self.model, "SolverDFSPH")
+        lib = _lib.load()
+        nw = int(lib.fs_context_worlds(ctx))
+        if nw <= 0:
+            raise RuntimeError("SolverDFSPH.last_world_iterations: the model's grid is not a batched WorldGrid")
+        infos = (_lib.DfsphInfo * nw)()
+        _lib.check(lib.fs_dfsph_info_worlds(ctx, infos, nw), "SolverDFSPH.last_world_iterations")
+        return [dict(rho_iterations=i.rho_iterations, vel_iterations=i.vel_iterations,
+                     density_residual=i.density_residual, divergence_residual=i.divergence_residual) for i in infos]
 
     def update_contacts(self, contacts) -> None:
         del contacts

@@ -188,9 +188,10 @@ int fs_grid_candidates(fs_context* ctx, const float* q, int64_t nq, float r, int
  * has its own tank: the walls of the step parameters are replaced by
  * fs_world_box.bound_* of the particle's world.  particle_world is required;
  * an index outside [0, nworlds) is clamped and raises FS_STATUS_BOUNDS.
- * WCSPH and PBF substeps and every separate pass accept a batched context;
- * fs_dfsph_substep, whose iteration decisions are global, returns
- * FS_ERR_INVALID.  fs_grid_build / fs_grid_candidates on a batched context
+ * Every substep and separate pass accepts a batched context.  The DFSPH
+ * substep takes its iteration decisions per world (each world iterates until
+ * the mean residual of its own dynamic particles passes, as that scene would
+ * alone); fs_dfsph_info_worlds reads them.  fs_grid_build / fs_grid_candidates on a batched context
  * (and the *_worlds forms on a hash-grid context) return FS_ERR_INVALID. */
 typedef struct {
   int32_t cell_lo[3];  /* cell coordinate int(x / h) of the box's first cell per axis */
@@ -218,6 +219,11 @@ int fs_wcsph_substep(fs_context* ctx, const fs_model* model, const fs_state* sta
 int fs_dfsph_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
                      const fs_dfsph_params* params, float* accel, fs_stream_t stream);
 int fs_dfsph_info_read(fs_context* ctx, fs_dfsph_info* info); /* synchronises the context's last stream */
+/* Per-world decisions of the last DFSPH substep of a batched context:
+ * info[w] for w < nworlds (nworlds = fs_context_worlds(ctx)); on a batched
+ * context fs_dfsph_info_read gives the largest iteration counts and residuals
+ * over the worlds.  Synchronises the context's last stream. */
+int fs_dfsph_info_worlds(fs_context* ctx, fs_dfsph_info* info, int32_t nworlds);
 /* SolverPBF.step (solver_pbf.py:676-954).  x_pred may be NULL (solver._x_pred [n][3]). */
 int fs_pbf_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
                    const fs_pbf_params* params, float* accel, float* x_pred, fs_stream_t stream);

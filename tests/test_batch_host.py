@@ -42,7 +42,9 @@ def test_default_batch_is_about_six_million_particles():
 
 
 def test_world_boxes_cover_each_tank():
-    """Every cell coordinate int(x / h) of a point of the tank lies in the box."""
+    """The cell coordinates int(x / h) of the tank's points span the box less
+    its one-cell margin; points up to one cell width outside the tank (where
+    DFSPH's mid-substep positions can lie) stay inside the box."""
     b = make_batch(n_scenes=8, seed=1)
     inv = np.float32(1.0) / np.float32(b.h)
     for s, (clo, dims, walls) in zip(b.scenes, b.boxes()):
@@ -51,7 +53,11 @@ def test_world_boxes_cover_each_tank():
         for k, (a, e) in enumerate(((-w, w), (-h, h), (0.0, 2.0 * l))):
             pts = np.linspace(a, e, 1001).astype(np.float32)
             c = np.trunc(pts * inv).astype(np.int64)
-            assert c.min() == clo[k] and c.max() == clo[k] + dims[k] - 1
+            assert c.min() == clo[k] + 1 and c.max() == clo[k] + dims[k] - 2
+            out = np.array([a - 0.999 * b.h, e + 0.999 * b.h], np.float32)
+            c = np.trunc(out * inv).astype(np.int64)
+            assert c.min() >= clo[k] and c.max() <= clo[k] + dims[k] - 1
+    assert all(d == tuple(x - 2 for x in dm) for (_, d, _), (_, dm, _) in zip(b.boxes(margin=0), b.boxes()))
 
 
 def test_shard_scenes_partitions_and_balances():

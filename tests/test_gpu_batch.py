@@ -8,7 +8,9 @@ Checked here:
     viscosity (the parity rule of the plain solvers: golden_io.compare_fields);
   - scenes overlapping in space do not interact;
   - a batched frame replayed from a CUDA graph equals the eager steps;
-  - the DFSPH substep refuses a batched context.
+  - a batched DFSPH substep takes its iteration decisions per world: every
+    scene iterates as it would alone (same counts, same bits), and the scenes
+    chosen here stop after different numbers of iterations.
 """
 
 import numpy as np
@@ -221,11 +223,119 @@ def test_batched_frame_graph_equals_eager(cuda_device):
     assert np.array_equal(res[0], res[1])
 
 
-def test_dfsph_substep_refuses_batched_context(cuda_device):
-    b = small_batch(n_scenes=2, seed=14)
-    m = batched_model(b, SolverDFSPH, device=cuda_device)
-    solver = SolverDFSPH(m, SolverDFSPH.SphConfig(particle_radius=b.radius, particle_length=b.spacing,
-                                                  smoothing_length_coff=2.0))
+# DFSPH with tolerances that the five scenes below (velocities scaled by
+# 0.5 (k + 1)) pass after different numbers of iterations: the oracle takes
+# 2, 2, 8, 8, 8 density and 8, 6, 8, 8, 8 divergence iterations on them.
+DFSPH_CFG = dict(COMMON, max_rho_iterations=8, max_vel_iterations=8, warm_start=False, max_kappa=1.0,
+                 max_kappa_v=100.0, eta_density=6.0, eta_divergence=48.0, min_neighbors_for_factor=8)
+
+
+def dfsph_batch():
+    b = small_batch(n_scenes=5, seed=14)
+    v = velocities(b, seed=8)
+    for k in range(len(b.scenes)):
+        v[b.starts[k]:b.starts[k + 1]] *= 0.5 * (k + 1)
+    return b, v
+
+
+def test_batched_dfsph_decides_per_world(cuda_device):
+    b, v = dfsph_batch()
+    cfg = dict(DFSPH_CFG, particle_radius=b.radius)
+    dt = 1e-3
+    m = batched_model(b, SolverDFSPH, device=cuda_device, v=v)
+    m.particle_q += torch.as_tensor(SHIFT, device=cuda_device)
+    solver = SolverDFSPH(m, SolverDFSPH.SphConfig(**cfg))
     s_in, s_out = m.state(), m.state()
-    with pytest.raises(RuntimeError, match="batched"):
-        solver.step(s_in, s_out, None, None, 1e-4)
+    solver.step(s_in, s_out, None, None, dt)
+    torch.cuda.synchronize()
+    assert m.particle_grid.status() == 0
+    per_world = solver.last_world_iterations()
+    got = dict(particle_q=s_out.particle_q.cpu().numpy(), particle_qd=s_out.particle_qd.cpu().numpy(),
+               accel=solver._particle_accel.cpu().numpy(),
+               **{k: t.cpu().numpy() for k, t in vars(s_out.sph).items()})
+    seen = set()
+    for k in range(len(b.scenes)):
+        model, state, walls, sl = scene_np(b, k, v)
+        c = dict(cfg, **walls)
+        alone, sv, _ = run_step("dfsph", model, state, c, dt, device=cuda_device)
+        it_alone = sv.last_iterations()
+        for key in ("rho_iterations", "vel_iterations"):
+            assert per_world[k][key] == it_alone[key], (k, key, per_world[k], it_alone)
+        for key in ("density_residual", "divergence_residual"):  # same terms, summed in another order
+            assert per_world[k][key] == pytest.approx(it_alone[key], rel=1e-12, abs=1e-12), (k, key)
+        for name in ("particle_q", "particle_qd", "accel"):
+            assert np.array_equal(alone[name], got[name][sl]), (k, name)
+        for name, val in alone["sph"].items():
+            assert np.array_equal(val, got[name][sl]), (k, name)
+        # the oracle's decisions and parity rule per scene
+        import oracle
+        _, _, info = oracle.dfsph_step(model, state, c, dt, precision="f32")
+        assert (info["rho_iterations"], info["vel_iterations"]) == (per_world[k]["rho_iterations"],
+                                                                    per_world[k]["vel_iterations"]), k
+        ref32 = oracle_outputs("dfsph", model, state, c, dt, "f32")
+        ref64 = oracle_outputs("dfsph", model, state, c, dt, "f64")
+        pairs = [(name, got[name][sl], val) for name, val in ref32.items()]
+        errors, _ = compare_fields(pairs, ref64)
+        assert not errors, f"scene {k}: " + "; ".join(errors)
+        seen.add((per_world[k]["rho_iterations"], per_world[k]["vel_iterations"]))
+    assert len(seen) > 1  # the worlds stopped at different iterations
+    total = solver.last_iterations()  # a batched context reports the largest counts
+    assert total["rho_iterations"] == max(w["rho_iterations"] for w in per_world)
+    assert total["vel_iterations"] == max(w["vel_iterations"] for w in per_world)
+
+
+def test_batched_dfsph_particles_past_the_walls_keep_bits(cuda_device):
+    """The wall layer at x = -W thrown outward at 20 m/s: DFSPH builds its
+    second grid from x + v* dt, before the walls act, and there particles of
+    three of the five scenes lie a cell past their tank.  The one-cell margin
+    of the world boxes keeps them in their own cells, so every scene still
+    equals its plain step bit for bit."""
+    b, v = dfsph_batch()
+    x = b.positions()
+    for k, s in enumerate(b.scenes):
+        a, e = b.starts[k], b.starts[k + 1]
+        edge = x[a:e, 0] < -s.walls[0] + b.spacing
+        v[a:e][edge, 0] = -20.0
+    cfg = dict(DFSPH_CFG, particle_radius=b.radius)
+    dt = 1e-3
+    m = batched_model(b, SolverDFSPH, device=cuda_device, v=v)
+    solver = SolverDFSPH(m, SolverDFSPH.SphConfig(**cfg))
+    s_in, s_out = m.state(), m.state()
+    solver.step(s_in, s_out, None, None, dt)
+    torch.cuda.synchronize()
+    assert m.particle_grid.status() == 0
+    vstar = s_out.sph.v_star.cpu().numpy()
+    inv = np.float32(1.0) / np.float32(b.h)
+    escaped = 0
+    for k, s in enumerate(b.scenes):
+        model, state, walls, sl = scene_np(b, k, v)
+        state["particle_q"] = x[sl]  # unshifted
+        mid = (x[sl] + vstar[sl] * np.float32(dt)).astype(np.float32)
+        escaped += int(np.sum(np.trunc(mid[:, 0] * inv) < int(np.float32(-s.walls[0]) * inv)))
+        alone, _, _ = run_step("dfsph", model, state, dict(cfg, **walls), dt, device=cuda_device)
+        assert np.array_equal(alone["particle_q"], s_out.particle_q[sl].cpu().numpy()), k
+        assert np.array_equal(alone["sph"]["neighbor_count"], s_out.sph.neighbor_count[sl].cpu().numpy()), k
+        assert np.array_equal(alone["sph"]["rho"], s_out.sph.rho[sl].cpu().numpy()), k
+    assert escaped > 0
+
+
+def test_batched_dfsph_frame_graph_equals_eager(cuda_device):
+    b, v = dfsph_batch()
+    cfg = dict(DFSPH_CFG, particle_radius=b.radius)
+    res = []
+    for graph in (False, True):
+        m = batched_model(b, SolverDFSPH, device=cuda_device, v=v)
+        solver = SolverDFSPH(m, SolverDFSPH.SphConfig(**cfg))
+        a, c = m.state(), m.state()
+        if graph:
+            fg = FrameGraph(solver, a, c, 1e-3, substeps=3, warmup=False)
+            out = fg.replay()
+        else:
+            for _ in range(3):
+                solver.step(a, c, None, None, 1e-3)
+                a, c = c, a
+            out = a
+        torch.cuda.synchronize()
+        res.append((out.particle_q.cpu().numpy(), solver.last_world_iterations()))
+    assert np.array_equal(res[0][0], res[1][0])
+    assert res[0][1] == res[1][1]
