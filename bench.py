@@ -177,23 +177,38 @@ def cpu_oracle_setup(name):
     return kind, model, state, asdict(solver_config(kind, s)), n
 
 
-def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1):
-    """Substeps of the CPU oracle until max_seconds have passed."""
+def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1, single_thread_seconds=8.0):
+    """Substeps of the CPU oracle until max_seconds have passed, on all host
+    threads; then (single_thread_seconds > 0) the same on one thread."""
     import oracle
-    kind, model, state, cfg, n = cpu_oracle_setup(name)
+    kind, model, state0, cfg, n = cpu_oracle_setup(name)
     step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step}[kind]
-    clock = HarnessClock(kind, cfg["particle_length"])
-    cores = oracle.num_threads(os.cpu_count() or 1)
-    k = 0
-    t0 = time.perf_counter()
-    while k < max_steps and (k < min_steps or time.perf_counter() - t0 < max_seconds):
-        out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
-        state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
-        k += 1
-    el = time.perf_counter() - t0
-    return dict(value=n * k / el, unit="particle-steps/s", cores=cores, kind="port",
-                sample=f"{k} consecutive substeps of the full {n}-particle workload in {el:.1f} s "
-                       f"(C++ restatement of the reference solver, OpenMP, {cores} threads)")
+
+    def run(seconds):
+        clock = HarnessClock(kind, cfg["particle_length"])
+        state, k = state0, 0
+        t0 = time.perf_counter()
+        while k < max_steps and (k < min_steps or time.perf_counter() - t0 < seconds):
+            out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
+            state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+            k += 1
+        return k, time.perf_counter() - t0
+
+    all_threads = os.cpu_count() or 1
+    cores = oracle.num_threads(all_threads)
+    k, el = run(max_seconds)
+    rec = dict(value=n * k / el, unit="particle-steps/s", cores=cores, kind="port",
+               sample=f"{k} consecutive substeps of the full {n}-particle workload in {el:.1f} s "
+                      f"(C++ restatement of the reference solver, OpenMP, {cores} threads)")
+    if single_thread_seconds > 0:
+        oracle.num_threads(1)
+        try:
+            k1, el1 = run(single_thread_seconds)
+        finally:
+            oracle.num_threads(all_threads)
+        rec["single_thread"] = dict(value=n * k1 / el1, cores=1,
+                                    sample=f"the first {k1} of those substeps on one thread in {el1:.1f} s")
+    return rec
 
 
 # ------------------------------------------------------ batched scenes ----

@@ -24,6 +24,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import snapshot
+
 # reference dam-break tank proportions and material (simulation.py:86-132)
 TANK = (1.2, 0.28, 0.6)
 REST_DENSITY = 1000.0
@@ -171,6 +173,59 @@ def scene_model(batch: Batch, k: int, solver_cls, device="cuda:0", v=None):
     return model_from_arrays(s.x, np.zeros_like(s.x) if v is None else v, batch.mass, device=device,
                              world=np.zeros(n, np.int32), gravity=[GRAVITY], radius=batch.radius, attributes=attrs,
                              solver_cls=solver_cls)
+
+
+# ------------------------------------------------------------ on disk ----
+def scene_table(batch: Batch) -> dict:
+    """The batch's per-scene parameters as ``scene_*`` arrays of a snapshot."""
+    sc = batch.scenes
+    return dict(scene_count=np.array([s.count for s in sc], np.int64),
+                scene_walls=np.array([s.walls for s in sc], np.float64).reshape(-1, 3),
+                scene_column_fraction=np.array([s.column_fraction for s in sc], np.float64),
+                scene_stiffness=np.array([s.stiffness for s in sc], np.float64),
+                scene_viscosity=np.array([s.viscosity for s in sc], np.float64),
+                scene_sha256=np.array([snapshot.positions_sha256(s.x) for s in sc]))
+
+
+def save_batch(path, batch: Batch, v=None, **meta) -> dict:
+    """Write a batch (its scenes' initial positions, optional velocities and
+    per-scene table) as a snapshot: the initial digest covers the whole
+    batch's positions, and ``scene_sha256`` each scene's own."""
+    x = batch.positions()
+    v = np.zeros_like(x) if v is None else v
+    return snapshot.save(path, x, v, None, batch.world(), initial_positions=x, extra_arrays=scene_table(batch),
+                         kind="batch", spacing=float(batch.spacing), scenes=len(batch.scenes), **meta)
+
+
+def save_batch_state(path, batch: Batch, model, state, **meta) -> dict:
+    """Snapshot of a batched model's state (a later frame) with the batch's
+    scene table and the digest of its initial positions."""
+    return snapshot.save_state(path, model, state, initial_positions=batch.positions(),
+                               extra_arrays=scene_table(batch), kind="batch_state", spacing=float(batch.spacing),
+                               scenes=len(batch.scenes), **meta)
+
+
+def load_batch(path) -> tuple:
+    """(Batch, Snapshot) from a file written by ``save_batch``; every
+    scene's positions are checked against its recorded digest."""
+    snap = snapshot.load(path)
+    if snap.meta.get("kind") != "batch":
+        raise ValueError(f"{path}: not a batch definition (kind {snap.meta.get('kind')!r})")
+    a = snap.arrays
+    counts = a["scene_count"]
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    b = Batch(spacing=float(snap.meta["spacing"]))
+    for k in range(len(counts)):
+        x = np.ascontiguousarray(snap.particle_q[starts[k]:starts[k + 1]])
+        if snapshot.positions_sha256(x) != str(a["scene_sha256"][k]):
+            raise ValueError(f"{path}: scene {k} positions do not match their digest")
+        b.scenes.append(Scene(count=int(counts[k]), walls=tuple(float(w) for w in a["scene_walls"][k]),
+                              column_fraction=float(a["scene_column_fraction"][k]),
+                              stiffness=float(a["scene_stiffness"][k]), viscosity=float(a["scene_viscosity"][k]),
+                              x=x))
+    if not snap.matches(b.positions()):
+        raise ValueError(f"{path}: batch positions do not match initial_position_sha256")
+    return b, snap
 
 
 def shard_scenes(counts, world_size: int) -> list:
