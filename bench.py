@@ -336,6 +336,42 @@ def time_batched(kind, dev, flush, frames=2, warm=1):
     return rec
 
 
+# ------------------------------------------------------------- metrics ----
+def time_metrics(dev, reps=20):
+    """The harness's per-frame metrics (simulation.py:198-225) on the WCSPH
+    dam break at 401,856 particles after one frame: reduced on the device
+    (fs_frame_metrics, 14 doubles read back) against the reference's way
+    (copy x, v, rho, p to the host and reduce with numpy).  Wall time per
+    call, both ending with the values on the host."""
+    import torch
+    from fluid_simulation_b200.dam_break import DamBreakSimulation
+    from fluid_simulation_b200.scene import make_scene
+    sim = DamBreakSimulation(make_scene(400000), "wcsph", device=dev)
+    sim.step()
+    torch.cuda.synchronize()
+
+    def wall(fn, k):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            out = fn()
+        return (time.perf_counter() - t0) / k * 1e3, out
+
+    t_dev, m_dev = wall(sim.metrics, reps)
+    t_host, m_host = wall(sim.metrics_host, max(3, reps // 4))
+    exact = ("speed_max", "height_min", "height_max", "density_min", "density_max", "density_p99", "pressure_min",
+             "pressure_max")
+    worst_mean = max(abs(m_dev[k] - m_host[k]) / max(abs(m_host[k]), 1e-30) for k in ("height_mean", "density_mean"))
+    rec = dict(workload="metrics_wcsph_dam_401856", particles=sim.scene.count, frame=sim.frame,
+               device_ms=round(t_dev, 4), host_numpy_ms=round(t_host, 3), speedup=round(t_host / t_dev, 1),
+               d2h_bytes_device=14 * 8, d2h_bytes_host=sim.scene.count * (12 + 12 + 4 + 4),
+               extrema_and_p99_equal=all(m_dev[k] == m_host[k] for k in exact), means_max_rel_diff=worst_mean)
+    del sim
+    torch.cuda.empty_cache()
+    return rec
+
+
 # ------------------------------------------------------------- adjoint ----
 def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
     """Differentiable WCSPH: forward of ``steps`` substeps (the plain drop-in
@@ -560,6 +596,8 @@ def run_ours(args):
         elif args.only == "frames":
             rec = [time_frame_loop(dev, flush), time_frame_loop(dev, flush, target=50000, frames=3),
                    time_frame_loop(dev, flush, frames=3, method="dfsph")]
+        elif args.only == "metrics":
+            rec = time_metrics(dev)
         else:
             rec = time_batched(args.only.split("_")[1], dev, flush, frames=1, warm=1)
         print(json.dumps(dict(only=args.only, record=rec)), flush=True)
@@ -717,6 +755,7 @@ def run_ours(args):
         secondary["wcsph_dam_frames_401856"] = time_frame_loop(dev, flush)
         secondary["wcsph_dam_frames_50232"] = time_frame_loop(dev, flush, target=50000, frames=3)
         secondary["dfsph_dam_frames_401856"] = time_frame_loop(dev, flush, frames=3, method="dfsph")
+        secondary["metrics_wcsph_dam_401856"] = time_metrics(dev)
     if world == 1 and not args.no_secondary and not args.no_adjoint:
         secondary["adjoint_wcsph_50232"] = time_adjoint(dev, flush)
         secondary["batched_adjoint_wcsph_256"] = time_adjoint(dev, flush, batched=True)
@@ -798,7 +837,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "batched_dfsph", "frames"],
+    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "batched_dfsph", "frames", "metrics"],
                     help="run one secondary workload alone (profiling); no bench line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

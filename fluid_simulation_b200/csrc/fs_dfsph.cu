@@ -345,8 +345,11 @@ __global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
 // Batched contexts: the residual of each world (block w sums the terms of
 // world w's slots, contiguous in cell order, in a fixed order) and its break
 // test (_density_residual / _divergence_residual, 579-596, per scene).
-__global__ void k_world_residual(GridDev g, const float* __restrict__ term, DfsphWorld* wctl, DfsphDev* gctl, int it,
-                                 float eta, const fs_frame_clock* clock) {
+constexpr int kWorldBlock = 512;  // threads per world of the residual pass
+
+__global__ void __launch_bounds__(kWorldBlock) k_world_residual(GridDev g, const float* __restrict__ term,
+                                                                DfsphWorld* wctl, DfsphDev* gctl, int it, float eta,
+                                                                const fs_frame_clock* clock) {
   if (gctl->done || clock_idle(clock)) return;
   const int w = blockIdx.x;
   DfsphWorld& W = wctl[w];
@@ -356,15 +359,25 @@ __global__ void k_world_residual(GridDev g, const float* __restrict__ term, Dfsp
   const int32_t s1 = g.off[box.base + box.dims[0] * box.dims[1] * box.dims[2]];
   double v = 0.0;
   long long c = 0;
-  for (int32_t s = s0 + (int32_t)threadIdx.x; s < s1; s += (int32_t)blockDim.x) {
-    const float t = __ldcg(term + s);
+  auto add = [&](float t) {
     if (t >= 0.f) {
       v += (double)t;
       c += 1;
     }
+  };
+  const int32_t step = (int32_t)blockDim.x;
+  int32_t s = s0 + (int32_t)threadIdx.x;
+  for (; s + 3 * step < s1; s += 4 * step) {  // four loads in flight, summed in slot order
+    const float t0 = __ldcg(term + s), t1 = __ldcg(term + s + step), t2 = __ldcg(term + s + 2 * step),
+                t3 = __ldcg(term + s + 3 * step);
+    add(t0);
+    add(t1);
+    add(t2);
+    add(t3);
   }
-  __shared__ double sd[kBlock / 32];
-  __shared__ long long sc[kBlock / 32];
+  for (; s < s1; s += step) add(__ldcg(term + s));
+  __shared__ double sd[kWorldBlock / 32];
+  __shared__ long long sc[kWorldBlock / 32];
   for (int o = 16; o > 0; o >>= 1) {
     v += __shfl_down_sync(0xffffffffu, v, o);
     c += __shfl_down_sync(0xffffffffu, c, o);
@@ -543,8 +556,8 @@ int run_rate(fs_context* c, const fs_model* m, int mode, int it, float h, float 
     PassScope ps_(c, P_DFSPH_RATE, st, per_world ? 2 : 1);
     k_rate<<<nb_blocks(c, a.n), c->nb_block, 0, st>>>(a);
     if (per_world)
-      k_world_residual<<<c->nworlds, kBlock, 0, st>>>(a.g, c->sc1b, c->dfsph_worlds + (ctrl - c->dfsph) * c->nworlds,
-                                                      ctrl, it, eta, c->clock);
+      k_world_residual<<<c->nworlds, kWorldBlock, 0, st>>>(a.g, c->sc1b, c->dfsph_worlds + (ctrl - c->dfsph) * c->nworlds,
+                                                           ctrl, it, eta, c->clock);
   }
   return launch_check("dfsph rate");
 }
