@@ -100,12 +100,14 @@ __global__ void FS_NB_BOUNDS k_density_factor(DensFactorArgs a) {
     const int cnt = record_list<true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
     const Cubic K(a.h);
     float rho = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sq = 0.f;
-    visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
+    visit_with<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true,
+                           [&](int t) { return make_float2(__ldg(a.mv + t), __ldg(&a.vs[t].w)); },
+                           [&](int t, float4 xj, const float2& mm) {  // (rest_density * volume, mass)
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       float r, rinv;
       r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-      rho = fmaf(__ldg(a.mv + t), K.w(r), rho);
-      const float gsc = __ldg(&a.vs[t].w) * K.grad_scale(r, rinv);
+      rho = fmaf(mm.x, K.w(r), rho);
+      const float gsc = mm.y * K.grad_scale(r, rinv);
       const float gx = gsc * dx, gy = gsc * dy, gz = gsc * dz;
       sgx += gx;
       sgy += gy;
@@ -155,13 +157,18 @@ __global__ void FS_NB_BOUNDS k_accel_predict(AccelArgs a) {
     const Cubic K(a.h);
     float ax = 0.f, ay = 0.f, az = 0.f;
     const bool lists_ok = a.use_lists && lists_usable(a.L);
-    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                        [&](int t, float4 xj) {
+    struct Nb {
+      float4 v;     // (v_j, m_j)
+      float rho;    // rho_j
+    };
+    visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                      [&](int t) { return Nb{__ldg(a.vs + t), __ldg(&a.sc2[t].x)}; },
+                      [&](int t, float4 xj, const Nb& nb) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       if (r2 == 0.f) return;  // zero vector d: every term vanishes
-      const float4 vj = __ldg(a.vs + t);
-      const float rho_j = __ldg(&a.sc2[t].x);
+      const float4 vj = nb.v;
+      const float rho_j = nb.rho;
       float r, rinv;
       r_and_inv(r2, r, rinv);
       const float wc = coh * vj.w * K.w(fmaxf(r, a.particle_radius));
@@ -441,12 +448,11 @@ __global__ void __launch_bounds__(kNbBlockMax, 4) k_correct(CorrectArgs a) {
       const float ci = a.kratio[s].x;
       float dvx = 0.f, dvy = 0.f, dvz = 0.f;
       const bool lists_ok = a.use_lists && lists_usable(a.L);
-      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                          [&](int t, float4 xj) {
+      visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t) { return __ldg(a.kratio + t); }, [&](int t, float4 xj, const float2& kj) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         float r, rinv;
         r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-        const float2 kj = __ldg(a.kratio + t);
         const float c = kj.y * (ci + kj.x) * K.grad_scale(r, rinv);
         dvx = fmaf(c, dx, dvx);
         dvy = fmaf(c, dy, dvy);

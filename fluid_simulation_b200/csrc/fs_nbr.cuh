@@ -201,6 +201,56 @@ FS_DEV void visit(const GridDev& g, const float4* __restrict__ xs, int s, float4
   }
 }
 
+// visit() for pair terms that read a second per-neighbour record (velocity,
+// kappa ratio, lambda ...): load(t) is issued together with the position
+// gather of each group of four list entries, so the two gathers of a
+// neighbour overlap instead of the second waiting for the distance test.
+// pair(t, xj, payload) is called in the same order and for the same entries
+// as visit() calls pair(t, xj).  Only for lists recorded at the current
+// positions (every entry within h2m except the particle itself), where the
+// early load fetches nothing that visit() would not.  FRESH as in visit().
+template <bool WITH_SELF, bool FRESH = false, class Load, class Pair>
+FS_DEV void visit_with(const GridDev& g, const float4* __restrict__ xs, int s, float4 xi, float h, float h2m,
+                       const NbrList& L, bool lists_ok, Load&& load, Pair&& pair) {
+  const int n = lists_ok ? (FRESH ? L.cnt[s] : __ldg(L.cnt + s)) : kNbMax + 1;
+  const bool use = n <= kNbMax;
+  if (g.tile_stats) {
+    const unsigned full = __activemask();
+    const unsigned b = __ballot_sync(full, use);
+    const unsigned bo = __ballot_sync(full, lists_ok && !use);
+    if ((int)(threadIdx.x & 31) == __ffs(full) - 1) {
+      atomicAdd(g.tile_stats, (unsigned long long)__popc(b));
+      atomicAdd(g.tile_stats + 1, (unsigned long long)__popc(full & ~b));
+      atomicAdd(g.tile_stats + 2, (unsigned long long)__popc(bo));
+    }
+  }
+  auto one = [&](int t, float4 xj, const auto& p) {
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    if (fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xj.w))) <= h2m && (WITH_SELF || t != s)) pair(t, xj, p);
+  };
+  if (use) {
+    const int32_t* col = L.idx + s;
+    auto entry = [&](int k) { return FRESH ? col[(int64_t)k * L.stride] : __ldg(col + (int64_t)k * L.stride); };
+    int k = 0;
+    for (; k + 3 < n; k += 4) {
+      const int t0 = entry(k), t1 = entry(k + 1), t2 = entry(k + 2), t3 = entry(k + 3);
+      const float4 x0 = __ldg(xs + t0), x1 = __ldg(xs + t1), x2 = __ldg(xs + t2), x3 = __ldg(xs + t3);
+      const auto p0 = load(t0), p1 = load(t1), p2 = load(t2), p3 = load(t3);
+      one(t0, x0, p0);
+      one(t1, x1, p1);
+      one(t2, x2, p2);
+      one(t3, x3, p3);
+    }
+    for (; k < n; ++k) {
+      const int t0 = entry(k);
+      const float4 x0 = __ldg(xs + t0);
+      one(t0, x0, load(t0));
+    }
+  } else {
+    scan_grid<WITH_SELF>(g, xs, s, xi, h, h2m, [&](int t, float4 xj) { pair(t, xj, load(t)); });
+  }
+}
+
 // Whether lists recorded for the current grid and positions exist.
 FS_DEV bool lists_usable(const NbrList& L) { return L.ctl->valid != 0; }
 

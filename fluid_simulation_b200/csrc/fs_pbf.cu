@@ -76,7 +76,11 @@ __global__ void FS_NB_BOUNDS_PBF k_density(GridDev g, NbrList L, int record, int
     if (pf_of(xi) & PF_ACTIVE) {
       if (record) {
         record_list<false>(g, xs, (int)s, xi, h, h2m, L);
-        visit<true, true>(g, xs, (int)s, xi, h, h2m, L, true, pair);
+        visit_with<true, true>(g, xs, (int)s, xi, h, h2m, L, true, [&](int t) { return __ldg(mv + t); },
+                               [&](int t, float4 xj, const float& m) {
+          const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+          acc = fmaf(m, K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz))), acc);
+        });
       } else {
         scan_grid<true>(g, xs, (int)s, xi, h, h2m, pair);
       }
@@ -125,11 +129,10 @@ __global__ void FS_NB_BOUNDS_PBF k_accel_apply(AccelArgs a) {
     float ax = 0.f, ay = 0.f, az = 0.f;
     if (gamma != 0.f || mu != 0.f) {
       const bool lists_ok = a.use_lists && lists_usable(a.L);
-      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                          [&](int t, float4 xj) {
+      visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t) { return __ldg(a.vs + t); }, [&](int t, float4 xj, const float4& vj) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float4 vj = __ldg(a.vs + t);
         float c = 0.f;
         if (gamma != 0.f) c -= coh * vj.w * K.w_r2(fmaxf(r2, rp2));  // W(max(r, r_p))
         if (mu != 0.f) {
@@ -191,13 +194,13 @@ __global__ void FS_NB_BOUNDS_PBF k_lambda(LambdaArgs a) {
     const float h2m = a.h * a.h * kSupportMargin;
     // records the lists the delta pass of this iteration (same positions) reuses
     record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
-    visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
+    visit_with<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t) { return __ldg(&a.vs[t].w); },
+                           [&](int t, float4 xj, const float& mj) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       if (t != (int)s && exact_lt_h(dx, dy, dz, a.h, K.h2)) ++cnt;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       float r, rinv;
       r_and_inv(r2, r, rinv);
-      const float mj = __ldg(&a.vs[t].w);
       rho = fmaf(mj, K.w_r2(r2), rho);
       const float c = -(mj * inv_rho0) * K.grad_scale(r, rinv);
       const float gjx = c * dx, gjy = c * dy, gjz = c * dz;
@@ -250,15 +253,14 @@ __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
     const float inv_wdq = scorr ? 1.0f / a.w_dq : 0.f;
     float dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
     const bool lists_ok = a.use_lists && lists_usable(a.L);
-    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                        [&](int t, float4 xj) {
+    visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                      [&](int t) { return __ldg(a.lam_s + t); }, [&](int t, float4 xj, const float2& lj) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       float r, rinv;
       r_and_inv(r2, r, rinv);
       float sc = 0.f;
       if (scorr) sc = -a.scorr_k * powf(K.w_r2(r2) * inv_wdq, a.scorr_n);
-      const float2 lj = __ldg(a.lam_s + t);
       const float c = (li + lj.x + sc) * lj.y * K.grad_scale(r, rinv);
       dx_ = fmaf(c, dx, dx_);
       dy_ = fmaf(c, dy, dy_);
@@ -328,10 +330,10 @@ __global__ void FS_NB_BOUNDS_PBF k_xsph_final(XsphArgs a) {
         const Poly6Spiky K(a.h);
         float cx = 0.f, cy = 0.f, cz = 0.f;
         const bool lists_ok = a.use_lists && lists_usable(a.L);
-        visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                            [&](int t, float4 xj) {
+        visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                          [&](int t) { return __ldg(a.vel + t); }, [&](int t, float4 xj, const float4& vj) {
           const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-          const float4 vj = __ldg(a.vel + t);  // (v, m / max(rho, 1e-6))
+          // vj = (v, m / max(rho, 1e-6))
           // (m_j / max(rho_j, 1e-6)) W(r), the ratio from the final density pass
           const float w = vj.w * K.w_r2(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
           cx = fmaf(vj.x - vi.x, w, cx);

@@ -80,11 +80,12 @@ __global__ void FS_NB_BOUNDS k_wcsph_density(DensityArgs a) {
     record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
     const Cubic K(a.h);
     float acc = 0.f;
-    visit<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t, float4 xj) {
+    visit_with<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t) { return __ldg(a.mv + t); },
+                           [&](int t, float4 xj, const float& m) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       float r, rinv;
       r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-      acc = fmaf(__ldg(a.mv + t), K.w(r), acc);
+      acc = fmaf(m, K.w(r), acc);
     });
     float p = a.stiffness[i] * (powf(acc / fmaxf(a.rest_density[i], 1.0e-6f), a.exponent[i]) - 1.0f);
     if (a.clamp) p = fmaxf(p, 0.f);
