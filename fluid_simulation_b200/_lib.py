@@ -43,7 +43,7 @@ class WorldBox(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("block_size", I32), ("particles_per_thread", I32), ("cell_ratio", F)]
+    _fields_ = [("block_size", I32), ("particles_per_thread", I32), ("cell_ratio", F), ("list_skin", F)]
 
 
 class FrameClock(C.Structure):
@@ -145,6 +145,7 @@ SIGNATURES = {
     "fs_timer_read": (C.c_int, [P, P, P, I32, P]),
     "fs_launch_count": (I64, [P]),
     "fs_list_stats": (C.c_int, [P, P, I32, I32]),
+    "fs_list_stats_enable": (C.c_int, [P, I32]),
     "fs_noalloc_max_particles": (I32, []),
     "fs_wcsph_density_noalloc": (C.c_int, [C.POINTER(Model), P, F, I32, P, P, P]),
     "fs_status_read": (C.c_int, [P, C.POINTER(C.c_uint32)]),

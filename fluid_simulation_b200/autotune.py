@@ -9,6 +9,10 @@ move that balance:
   particles_per_thread  cell-sorted particles each thread walks (1, 2, 4)
   cell_ratio            grid cell width / h (WCSPH only: 1 or 0.5)
 
+(a fourth, ``list_skin``, the skin of PBF's first density lists that lets
+the first lambda pass skip its grid scan, changes no result either and
+keeps its default here).
+
 ``autotune(solver, state, dt)`` times a few substeps from one saved state
 under every candidate (each candidate starts from the same state, so DFSPH
 runs the same iterations), keeps the fastest on the solver's context and
@@ -38,16 +42,19 @@ class Tuning:
     block_size: int = 128
     particles_per_thread: int = 1
     cell_ratio: float = 1.0
+    list_skin: float = 0.02
 
 
 def get_tuning(ctx) -> Tuning:
     t = _lib.Tuning()
     _lib.check(_lib.load().fs_context_get_tuning(ctx, C.byref(t)), "fs_context_get_tuning")
-    return Tuning(int(t.block_size), int(t.particles_per_thread), float(t.cell_ratio))
+    f32 = lambda v: float(f"{v:.7g}")  # the decimal a float32 field was set from
+    return Tuning(int(t.block_size), int(t.particles_per_thread), f32(t.cell_ratio), f32(t.list_skin))
 
 
 def set_tuning(ctx, tuning: Tuning) -> None:
-    t = _lib.Tuning(int(tuning.block_size), int(tuning.particles_per_thread), float(tuning.cell_ratio))
+    t = _lib.Tuning(int(tuning.block_size), int(tuning.particles_per_thread), float(tuning.cell_ratio),
+                    float(tuning.list_skin))
     _lib.check(_lib.load().fs_context_set_tuning(ctx, C.byref(t)), "fs_context_set_tuning")
 
 

@@ -234,7 +234,7 @@ GridDev grid_view(const fs_context* c) {
   g.mask_y = pow2mask(g.dim_y);
   g.mask_z = pow2mask(g.dim_z);
   g.inv = c->built_inv;
-  g.tile_stats = c->tile_stats;
+  g.tile_stats = c->stats_on ? c->tile_stats : nullptr;
   g.worlds = c->worlds;
   g.nworlds = c->nworlds;
   return g;
@@ -396,9 +396,12 @@ int fs_context_set_tuning(fs_context* c, const fs_tuning* t) {
     return set_error(FS_ERR_INVALID, "fs_context_set_tuning: cell_ratio must be 1 or 0.5");
   if (c->worlds && t->cell_ratio != 1.0f)
     return set_error(FS_ERR_INVALID, "fs_context_set_tuning: batched contexts bin in cells of width h");
+  if (!(t->list_skin >= 0.f && t->list_skin <= 0.25f))
+    return set_error(FS_ERR_INVALID, "fs_context_set_tuning: list_skin must lie in [0, 0.25]");
   c->nb_block = t->block_size;
   c->nb_ppt = t->particles_per_thread;
   c->cell_ratio = t->cell_ratio;
+  c->list_skin = t->list_skin;
   return FS_OK;
 }
 
@@ -407,6 +410,7 @@ int fs_context_get_tuning(const fs_context* c, fs_tuning* t) {
   t->block_size = c->nb_block;
   t->particles_per_thread = c->nb_ppt;
   t->cell_ratio = c->cell_ratio;
+  t->list_skin = c->list_skin;
   return FS_OK;
 }
 
@@ -437,6 +441,7 @@ static int context_alloc(fs_context* c, int64_t capacity, int64_t ncell) {
       {(void**)&c->xo_tmp, sizeof(float) * 3 * cap},    {(void**)&c->vo_tmp, sizeof(float) * 3 * cap},
       {(void**)&c->red_part, sizeof(double) * rb},      {(void**)&c->red_cnt, sizeof(int64_t) * rb},
       {(void**)&c->dfsph, sizeof(DfsphDev) * 2},         {(void**)&c->status, sizeof(uint32_t)},
+      {(void**)&c->pbf_disp, sizeof(uint32_t)},
       {(void**)&c->tile_stats, sizeof(unsigned long long) * 8},
       {(void**)&c->nb_idx, sizeof(int32_t) * kNbMax * cap},  {(void**)&c->nb_cnt, sizeof(int32_t) * cap},
       {(void**)&c->nb_ctl, sizeof(ListCtl)},
@@ -470,7 +475,7 @@ int fs_context_destroy(fs_context* c) {
   void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
                 c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->krm, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
                 c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds, c->metrics,
-                c->dfsph_worlds};
+                c->dfsph_worlds, c->pbf_disp};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete c;
@@ -637,6 +642,12 @@ int fs_list_stats(fs_context* c, int64_t* counters, int32_t ncounters, int32_t r
   for (int k = 0; k < ncounters && k < 8; ++k) counters[k] = (int64_t)h[k];
   if (reset) rc = check_cuda(cudaMemset(c->tile_stats, 0, sizeof(h)), "fs_list_stats: reset");
   return rc;
+}
+
+int fs_list_stats_enable(fs_context* c, int32_t on) {
+  if (!c) return set_error(FS_ERR_INVALID, "fs_list_stats_enable: null context");
+  c->stats_on = on != 0;
+  return FS_OK;
 }
 
 int fs_status_clear(fs_context* c, fs_stream_t stream) {

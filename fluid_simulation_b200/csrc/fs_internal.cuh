@@ -66,7 +66,7 @@ struct GridDev {
   int32_t dim_x, dim_y, dim_z, rounding;
   int32_t mask_x, mask_y, mask_z;  // dim - 1 when the dim is a power of two, else -1
   float inv;            // 1 / cell width, float32 as warp
-  unsigned long long* tile_stats;  // [2]: neighbour visits served by lists / by grid rescans
+  unsigned long long* tile_stats;  // list counters (fs_list_stats), null while counting is off
 };
 
 }  // namespace fs
@@ -109,7 +109,9 @@ struct fs_context {
   fs::DfsphDev* dfsph = nullptr; // [2] control blocks (density half, divergence half)
   fs::DfsphWorld* dfsph_worlds = nullptr;  // batched contexts: [2][nworlds] per-world decisions
   uint32_t* status = nullptr;
-  unsigned long long* tile_stats = nullptr;  // [2] visits served by lists / by rescans
+  uint32_t* pbf_disp = nullptr;  // PBF: largest displacement (float bits) since the lists' recording
+  unsigned long long* tile_stats = nullptr;  // [4] list counters (fs_list_stats)
+  bool stats_on = false;                     // count them (fs_list_stats_enable)
 
   // neighbour lists (fs_nbr.cuh)
   int32_t* nb_idx = nullptr;     // [kNbMax][cap]
@@ -131,6 +133,7 @@ struct fs_context {
   int32_t nb_block = 128;      // threads per block: 64, 128 or 256
   int32_t nb_ppt = 1;          // particles per thread: 1, 2 or 4
   float cell_ratio = 1.f;      // WCSPH grid cell width / h: 1 or 1/2
+  float list_skin = 0.02f;     // PBF first-density list skin / h (0: the first lambda pass scans)
 
   // instrumentation
   fs::PassTimer timer;
@@ -351,19 +354,54 @@ FS_DEV int world_cell_key(const WorldDev& W, float inv, float px, float py, floa
   return W.base + (cz * W.dims[1] + cy) * W.dims[0] + cx;
 }
 
+// The cells a query at p with radius r visits: [x0, x1] x [y0, y1] x [z0, z1]
+// in the world's box coordinates (batched contexts) or in unwrapped hash-grid
+// cell coordinates (wrapped modulo the dims when visited).
+struct QueryBox {
+  int x0, x1, y0, y1, z0, z1;
+};
+
+FS_DEV QueryBox query_box_world(const GridDev& g, const WorldDev& W, float px, float py, float pz, float r) {
+  auto cell = [&](float v, int k) { return world_axis_cell(v, g.inv, W.clo[k], W.dims[k]); };
+  return QueryBox{cell(__fsub_rn(px, r), 0), cell(__fadd_rn(px, r), 0), cell(__fsub_rn(py, r), 1),
+                  cell(__fadd_rn(py, r), 1), cell(__fsub_rn(pz, r), 2), cell(__fadd_rn(pz, r), 2)};
+}
+
+FS_DEV QueryBox query_box_hash(const GridDev& g, float px, float py, float pz, float r) {
+  QueryBox b;
+  b.x0 = to_cell(__fmul_rn(__fsub_rn(px, r), g.inv), g.rounding);
+  b.y0 = to_cell(__fmul_rn(__fsub_rn(py, r), g.inv), g.rounding);
+  b.z0 = to_cell(__fmul_rn(__fsub_rn(pz, r), g.inv), g.rounding);
+  b.x1 = min(to_cell(__fmul_rn(__fadd_rn(px, r), g.inv), g.rounding), b.x0 + g.dim_x - 1);
+  b.y1 = min(to_cell(__fmul_rn(__fadd_rn(py, r), g.inv), g.rounding), b.y0 + g.dim_y - 1);
+  b.z1 = min(to_cell(__fmul_rn(__fadd_rn(pz, r), g.inv), g.rounding), b.z0 + g.dim_z - 1);
+  return b;
+}
+
+// Whether queries at p and q (same world w) visit the same cells.
+FS_DEV bool same_query_cells(const GridDev& g, int w, float4 p, float4 q, float r) {
+  QueryBox a, b;
+  if (g.worlds) {
+    const WorldDev& W = g.worlds[world_index(w, g.nworlds)];
+    a = query_box_world(g, W, p.x, p.y, p.z, r);
+    b = query_box_world(g, W, q.x, q.y, q.z, r);
+  } else {
+    a = query_box_hash(g, p.x, p.y, p.z, r);
+    b = query_box_hash(g, q.x, q.y, q.z, r);
+  }
+  return a.x0 == b.x0 && a.x1 == b.x1 && a.y0 == b.y0 && a.y1 == b.y1 && a.z0 == b.z0 && a.z1 == b.z1;
+}
+
 // The query cells of world w in the order z-outer, y, x-inner; each row of
 // x cells is one contiguous slot range, passed to rf(first, end).
 template <class RF>
 FS_DEV void for_each_range_world(const GridDev& g, int w, float px, float py, float pz, float r, RF&& rf) {
   const WorldDev& W = g.worlds[world_index(w, g.nworlds)];
-  auto cell = [&](float v, int k) { return world_axis_cell(v, g.inv, W.clo[k], W.dims[k]); };
-  const int x0 = cell(__fsub_rn(px, r), 0), x1 = cell(__fadd_rn(px, r), 0);
-  const int y0 = cell(__fsub_rn(py, r), 1), y1 = cell(__fadd_rn(py, r), 1);
-  const int z0 = cell(__fsub_rn(pz, r), 2), z1 = cell(__fadd_rn(pz, r), 2);
-  for (int z = z0; z <= z1; ++z)
-    for (int y = y0; y <= y1; ++y) {
+  const QueryBox b = query_box_world(g, W, px, py, pz, r);
+  for (int z = b.z0; z <= b.z1; ++z)
+    for (int y = b.y0; y <= b.y1; ++y) {
       const int row = W.base + (z * W.dims[1] + y) * W.dims[0];
-      rf(__ldg(g.off + row + x0), __ldg(g.off + row + x1 + 1));
+      rf(__ldg(g.off + row + b.x0), __ldg(g.off + row + b.x1 + 1));
     }
 }
 
@@ -374,12 +412,8 @@ FS_DEV void for_each_range_world(const GridDev& g, int w, float px, float py, fl
 // run that wraps modulo dim_x splits in two.
 template <class RF>
 FS_DEV void for_each_range_hash(const GridDev& g, float px, float py, float pz, float r, RF&& rf) {
-  const int x0 = to_cell(__fmul_rn(__fsub_rn(px, r), g.inv), g.rounding);
-  const int y0 = to_cell(__fmul_rn(__fsub_rn(py, r), g.inv), g.rounding);
-  const int z0 = to_cell(__fmul_rn(__fsub_rn(pz, r), g.inv), g.rounding);
-  const int x1 = min(to_cell(__fmul_rn(__fadd_rn(px, r), g.inv), g.rounding), x0 + g.dim_x - 1);
-  const int y1 = min(to_cell(__fmul_rn(__fadd_rn(py, r), g.inv), g.rounding), y0 + g.dim_y - 1);
-  const int z1 = min(to_cell(__fmul_rn(__fadd_rn(pz, r), g.inv), g.rounding), z0 + g.dim_z - 1);
+  const QueryBox b = query_box_hash(g, px, py, pz, r);
+  const int x0 = b.x0, x1 = b.x1, y0 = b.y0, y1 = b.y1, z0 = b.z0, z1 = b.z1;
   const int nx = x1 - x0 + 1;
   const int xa = x0 + (1 << 20);
   for (int z = z0; z <= z1; ++z) {

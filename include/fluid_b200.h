@@ -149,12 +149,19 @@ int64_t fs_context_capacity(const fs_context* ctx);
  *                         DFSPH always bin at h: PBF queries the grid from
  *                         moved positions and DFSPH counts candidates, so
  *                         the cell width is part of their results.
- * block_size and particles_per_thread change no result (DFSPH sums its
- * residual per block, so its last bits follow block_size). */
+ *   list_skin             PBF: the first density pass records its neighbour
+ *                         lists out to h (1 + list_skin) (default 0.02, at
+ *                         most 0.25), so that the first lambda pass, after
+ *                         the non-pressure update moved every particle by
+ *                         less than list_skin h / 2, reuses them instead of
+ *                         scanning the grid; 0 always scans.
+ * block_size, particles_per_thread and list_skin change no result (DFSPH
+ * sums its residual per block, so its last bits follow block_size). */
 typedef struct {
   int32_t block_size;
   int32_t particles_per_thread;
   float cell_ratio;
+  float list_skin;
 } fs_tuning;
 int fs_context_set_tuning(fs_context* ctx, const fs_tuning* tuning);
 int fs_context_get_tuning(const fs_context* ctx, fs_tuning* tuning);
@@ -374,8 +381,12 @@ int fs_timer_read(fs_context* ctx, float* ms_per_pass, int32_t* launches_per_pas
 int64_t fs_launch_count(const fs_context* ctx);           /* kernels launched through ctx so far */
 /* Neighbour-list counters since the last reset (synchronises): [0] particle
  * visits served by recorded lists, [1] visits that scanned the grid, [2] of
- * those, scans because a recorded list overflowed. */
+ * those, scans because a recorded list overflowed, [3] PBF first-lambda
+ * passes that reused the first density's list instead of scanning.  Counted
+ * only while enabled (fs_list_stats_enable; off by default: the counting
+ * adds atomics to every neighbour pass). */
 int fs_list_stats(fs_context* ctx, int64_t* counters, int32_t ncounters, int32_t reset);
+int fs_list_stats_enable(fs_context* ctx, int32_t on);
 
 /* ---- allocation-free density (no counterpart in the reference) ----------
  * For callers that cannot allocate device memory (hosts whose allocator

@@ -54,6 +54,38 @@ def test_block_size_and_particles_per_thread_change_no_result(kind, cuda_device)
             assert torch.equal(got[k], ref[k]), (t, k)
 
 
+def test_pbf_list_skin_changes_no_result(cuda_device):
+    """The first lambda pass reuses the first density's lists when every
+    particle moved less than list_skin h / 2 in between.  Skin off, default
+    and largest: the same bits.  With a strong cohesion the non-pressure
+    update moves particles past the skin and the device falls back to
+    scanning: the same bits again, and no reuse counted."""
+    lib = _lib.load()
+    for gamma in (0.0, 1.0):
+        s, m, solver, dt = setup("pbf", cuda_device)
+        if gamma:
+            m.sph.surface_tension.fill_(gamma)
+        ctx = m.particle_grid._ctx
+        _lib.check(lib.fs_list_stats_enable(ctx, 1), "stats")
+        counters = (C.c_int64 * 4)()
+        outs, reused = {}, {}
+        for skin in (0.0, 0.02, 0.25):
+            set_tuning(ctx, Tuning(128, 1, 1.0, skin))
+            _lib.check(lib.fs_list_stats(ctx, counters, 4, 1), "stats")
+            outs[skin] = step_outputs(m, solver, dt)
+            _lib.check(lib.fs_list_stats(ctx, counters, 4, 1), "stats")
+            reused[skin] = counters[3]
+        for skin in (0.02, 0.25):
+            for k in outs[0.0]:
+                assert torch.equal(outs[skin][k], outs[0.0][k]), (gamma, skin, k)
+        assert reused[0.0] == 0
+        if gamma == 0.0:
+            assert reused[0.02] > 0.9 * s.count, reused
+        else:
+            assert reused[0.02] == 0, reused
+        _lib.check(lib.fs_list_stats_enable(ctx, 0), "stats")
+
+
 def test_wcsph_half_cells_keep_parity(cuda_device):
     s, m, solver, dt = setup("wcsph", cuda_device, target=10000)
     set_tuning(m.particle_grid._ctx, Tuning(128, 1, 0.5))
@@ -81,7 +113,8 @@ def test_wcsph_half_cells_keep_parity(cuda_device):
 def test_invalid_tunings_are_refused(cuda_device):
     _, m, _, _ = setup("pbf", cuda_device, target=3000)
     lib = _lib.load()
-    for bad in ((96, 1, 1.0), (128, 3, 1.0), (128, 1, 0.7)):
+    for bad in ((96, 1, 1.0, 0.02), (128, 3, 1.0, 0.02), (128, 1, 0.7, 0.02), (128, 1, 1.0, -0.1),
+                (128, 1, 1.0, 0.3)):
         rc = lib.fs_context_set_tuning(m.particle_grid._ctx, C.byref(_lib.Tuning(*bad)))
         assert rc == _lib.FS_ERR_INVALID
     b = make_batch(n_scenes=2, seed=1, n_lo=1000, n_hi=2000)
