@@ -307,12 +307,11 @@ __global__ void FS_NB_BOUNDS k_rate(RateArgs a) {
       const float4 vi = a.vstar[s];
       const Cubic K(a.h);
       const bool lists_ok = a.use_lists && lists_usable(a.L);
-      visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                          [&](int t, float4 xj) {
+      visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t) { return __ldg(a.vstar + t); }, [&](int t, float4 xj, const float4& vj) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         float r, rinv;
         r_and_inv(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), r, rinv);
-        const float4 vj = __ldg(a.vstar + t);
         const float vdot = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
         d = fmaf(vj.w * K.grad_scale(r, rinv), vdot, d);
       });

@@ -632,11 +632,28 @@ int fs_status_read(fs_context* c, uint32_t* status) {
   return check_cuda(cudaStreamSynchronize(c->last_stream), "fs_status_read: sync");
 }
 
+// tallies the current lists: [0] usable, [1] overflowed (their particles rescan)
+__global__ void k_list_tally(int64_t n, const int32_t* __restrict__ cnt, unsigned long long* out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = s < n && cnt[s] <= kNbMax, over = s < n && cnt[s] > kNbMax;
+  const unsigned a = __ballot_sync(0xffffffffu, ok), b = __ballot_sync(0xffffffffu, over);
+  if ((threadIdx.x & 31) == 0) {
+    if (a) atomicAdd(out, (unsigned long long)__popc(a));
+    if (b) atomicAdd(out + 1, (unsigned long long)__popc(b));
+  }
+}
+
 int fs_list_stats(fs_context* c, int64_t* counters, int32_t ncounters, int32_t reset) {
   if (!c || !counters || ncounters < 0) return set_error(FS_ERR_INVALID, "fs_list_stats: bad arguments");
   DeviceGuard dg(c->device);
   unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int rc = check_cuda(cudaStreamSynchronize(c->last_stream), "fs_list_stats: sync");
+  if (!rc) rc = check_cuda(cudaMemset(c->tile_stats, 0, 2 * sizeof(unsigned long long)), "fs_list_stats: clear");
+  const int64_t n = c->built_n > 0 ? c->built_n : 0;
+  if (!rc && n > 0) {
+    k_list_tally<<<blocks_for(n), kBlock>>>(n, c->nb_cnt, c->tile_stats);
+    rc = launch_check("fs_list_stats");
+  }
   if (!rc) rc = check_cuda(cudaMemcpy(h, c->tile_stats, sizeof(h), cudaMemcpyDeviceToHost), "fs_list_stats");
   if (rc) return rc;
   for (int k = 0; k < ncounters && k < 8; ++k) counters[k] = (int64_t)h[k];

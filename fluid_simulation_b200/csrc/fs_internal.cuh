@@ -110,7 +110,7 @@ struct fs_context {
   fs::DfsphWorld* dfsph_worlds = nullptr;  // batched contexts: [2][nworlds] per-world decisions
   uint32_t* status = nullptr;
   uint32_t* pbf_disp = nullptr;  // PBF: largest displacement (float bits) since the lists' recording
-  unsigned long long* tile_stats = nullptr;  // [4] list counters (fs_list_stats)
+  unsigned long long* tile_stats = nullptr;  // list counters (fs_list_stats)
   bool stats_on = false;                     // count them (fs_list_stats_enable)
 
   // neighbour lists (fs_nbr.cuh)

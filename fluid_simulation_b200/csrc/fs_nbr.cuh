@@ -166,16 +166,6 @@ FS_DEV void visit(const GridDev& g, const float4* __restrict__ xs, int s, float4
                   const NbrList& L, bool lists_ok, Pair&& pair) {
   const int n = lists_ok ? (FRESH ? L.cnt[s] : __ldg(L.cnt + s)) : kNbMax + 1;
   const bool use = n <= kNbMax;
-  if (g.tile_stats) {  // visits served by lists / by rescans / rescans of an overflowed list
-    const unsigned full = __activemask();
-    const unsigned b = __ballot_sync(full, use);
-    const unsigned bo = __ballot_sync(full, lists_ok && !use);
-    if ((int)(threadIdx.x & 31) == __ffs(full) - 1) {
-      atomicAdd(g.tile_stats, (unsigned long long)__popc(b));
-      atomicAdd(g.tile_stats + 1, (unsigned long long)__popc(full & ~b));
-      atomicAdd(g.tile_stats + 2, (unsigned long long)__popc(bo));
-    }
-  }
   if (use) {
     const int32_t* col = L.idx + s;
     auto entry = [&](int k) { return FRESH ? col[(int64_t)k * L.stride] : __ldg(col + (int64_t)k * L.stride); };
@@ -214,16 +204,6 @@ FS_DEV void visit_with(const GridDev& g, const float4* __restrict__ xs, int s, f
                        const NbrList& L, bool lists_ok, Load&& load, Pair&& pair) {
   const int n = lists_ok ? (FRESH ? L.cnt[s] : __ldg(L.cnt + s)) : kNbMax + 1;
   const bool use = n <= kNbMax;
-  if (g.tile_stats) {
-    const unsigned full = __activemask();
-    const unsigned b = __ballot_sync(full, use);
-    const unsigned bo = __ballot_sync(full, lists_ok && !use);
-    if ((int)(threadIdx.x & 31) == __ffs(full) - 1) {
-      atomicAdd(g.tile_stats, (unsigned long long)__popc(b));
-      atomicAdd(g.tile_stats + 1, (unsigned long long)__popc(full & ~b));
-      atomicAdd(g.tile_stats + 2, (unsigned long long)__popc(bo));
-    }
-  }
   auto one = [&](int t, float4 xj, const auto& p) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
     if (fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xj.w))) <= h2m && (WITH_SELF || t != s)) pair(t, xj, p);

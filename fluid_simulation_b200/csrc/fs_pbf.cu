@@ -221,7 +221,7 @@ __global__ void FS_NB_BOUNDS_PBF k_lambda(LambdaArgs a) {
     if (a.g.tile_stats && a.xs_rec) {
       const unsigned full = __activemask();
       const unsigned b = __ballot_sync(full, reuse);
-      if ((int)(threadIdx.x & 31) == __ffs(full) - 1) atomicAdd(a.g.tile_stats + 3, (unsigned long long)__popc(b));
+      if ((int)(threadIdx.x & 31) == __ffs(full) - 1) atomicAdd(a.g.tile_stats + 2, (unsigned long long)__popc(b));
     }
     if (!reuse) record_list<false>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L);
     visit_with<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t) { return __ldg(&a.vs[t].w); },

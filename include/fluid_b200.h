@@ -379,12 +379,12 @@ const char* fs_pass_name(int32_t pass);
 int fs_timer_enable(fs_context* ctx, int32_t capacity); /* capacity 0 frees the events */
 int fs_timer_read(fs_context* ctx, float* ms_per_pass, int32_t* launches_per_pass, int32_t npass, int32_t* dropped);
 int64_t fs_launch_count(const fs_context* ctx);           /* kernels launched through ctx so far */
-/* Neighbour-list counters since the last reset (synchronises): [0] particle
- * visits served by recorded lists, [1] visits that scanned the grid, [2] of
- * those, scans because a recorded list overflowed, [3] PBF first-lambda
- * passes that reused the first density's list instead of scanning.  Counted
- * only while enabled (fs_list_stats_enable; off by default: the counting
- * adds atomics to every neighbour pass). */
+/* Neighbour-list counters (synchronises): [0] particles whose current list
+ * is usable, [1] particles whose current list overflowed (kNbMax entries;
+ * their later passes scan the grid), both tallied from the lists now held;
+ * [2] PBF first-lambda passes that reused the first density's list instead
+ * of scanning, since the last reset and only while enabled
+ * (fs_list_stats_enable, off by default). */
 int fs_list_stats(fs_context* ctx, int64_t* counters, int32_t ncounters, int32_t reset);
 int fs_list_stats_enable(fs_context* ctx, int32_t on);
 

@@ -67,14 +67,15 @@ def test_pbf_list_skin_changes_no_result(cuda_device):
             m.sph.surface_tension.fill_(gamma)
         ctx = m.particle_grid._ctx
         _lib.check(lib.fs_list_stats_enable(ctx, 1), "stats")
-        counters = (C.c_int64 * 4)()
+        counters = (C.c_int64 * 3)()
         outs, reused = {}, {}
         for skin in (0.0, 0.02, 0.25):
             set_tuning(ctx, Tuning(128, 1, 1.0, skin))
-            _lib.check(lib.fs_list_stats(ctx, counters, 4, 1), "stats")
+            _lib.check(lib.fs_list_stats(ctx, counters, 3, 1), "stats")
             outs[skin] = step_outputs(m, solver, dt)
-            _lib.check(lib.fs_list_stats(ctx, counters, 4, 1), "stats")
-            reused[skin] = counters[3]
+            _lib.check(lib.fs_list_stats(ctx, counters, 3, 1), "stats")
+            assert counters[0] + counters[1] == s.count  # the XSPH lists of the final density
+            reused[skin] = counters[2]
         for skin in (0.02, 0.25):
             for k in outs[0.0]:
                 assert torch.equal(outs[skin][k], outs[0.0][k]), (gamma, skin, k)
