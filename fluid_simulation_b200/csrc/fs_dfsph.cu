@@ -157,18 +157,13 @@ __global__ void FS_NB_BOUNDS k_accel_predict(AccelArgs a) {
     const Cubic K(a.h);
     float ax = 0.f, ay = 0.f, az = 0.f;
     const bool lists_ok = a.use_lists && lists_usable(a.L);
-    struct Nb {
-      float4 v;     // (v_j, m_j)
-      float rho;    // rho_j
-    };
-    visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
-                      [&](int t) { return Nb{__ldg(a.vs + t), __ldg(&a.sc2[t].x)}; },
-                      [&](int t, float4 xj, const Nb& nb) {
+    visit<false, false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+                        [&](int t, float4 xj) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       if (r2 == 0.f) return;  // zero vector d: every term vanishes
-      const float4 vj = nb.v;
-      const float rho_j = nb.rho;
+      const float4 vj = __ldg(a.vs + t);
+      const float rho_j = __ldg(&a.sc2[t].x);
       float r, rinv;
       r_and_inv(r2, r, rinv);
       const float wc = coh * vj.w * K.w(fmaxf(r, a.particle_radius));
