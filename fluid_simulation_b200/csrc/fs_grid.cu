@@ -300,6 +300,19 @@ int check_cuda(cudaError_t e, const char* what) {
 int launch_check(const char* what) { return check_cuda(cudaGetLastError(), what); }
 }  // namespace fs
 
+namespace fs {
+// tallies the current lists: [0] usable, [1] overflowed (their particles rescan)
+__global__ void k_list_tally(int64_t n, const int32_t* __restrict__ cnt, unsigned long long* out) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = s < n && cnt[s] <= kNbMax, over = s < n && cnt[s] > kNbMax;
+  const unsigned a = __ballot_sync(0xffffffffu, ok), b = __ballot_sync(0xffffffffu, over);
+  if ((threadIdx.x & 31) == 0) {
+    if (a) atomicAdd(out, (unsigned long long)__popc(a));
+    if (b) atomicAdd(out + 1, (unsigned long long)__popc(b));
+  }
+}
+}  // namespace fs
+
 extern "C" {
 
 const char* fs_last_error_string(void) { return fs::g_err; }
@@ -630,17 +643,6 @@ int fs_status_read(fs_context* c, uint32_t* status) {
                       "fs_status_read");
   if (rc) return rc;
   return check_cuda(cudaStreamSynchronize(c->last_stream), "fs_status_read: sync");
-}
-
-// tallies the current lists: [0] usable, [1] overflowed (their particles rescan)
-__global__ void k_list_tally(int64_t n, const int32_t* __restrict__ cnt, unsigned long long* out) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool ok = s < n && cnt[s] <= kNbMax, over = s < n && cnt[s] > kNbMax;
-  const unsigned a = __ballot_sync(0xffffffffu, ok), b = __ballot_sync(0xffffffffu, over);
-  if ((threadIdx.x & 31) == 0) {
-    if (a) atomicAdd(out, (unsigned long long)__popc(a));
-    if (b) atomicAdd(out + 1, (unsigned long long)__popc(b));
-  }
 }
 
 int fs_list_stats(fs_context* c, int64_t* counters, int32_t ncounters, int32_t reset) {
