@@ -647,6 +647,8 @@ def run_ours(args):
         ev[k][1].record()
         flush.zero_()
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     launches = lib.fs_launch_count(ctx) - launches0
     clk = clocks.stop()
     ms = (C.c_float * npass)()
