@@ -129,7 +129,7 @@ def test_viscous_timestep_damps_velocity_and_completes_frame(cuda_device):
     assert np.sum(sim.state_0.particle_qd.cpu().numpy() ** 2) < np.sum(velocity ** 2)
 
 
-@pytest.mark.parametrize("method", ["wcsph", "pbf"])
+@pytest.mark.parametrize("method", ["wcsph", "pbf", "dfsph"])
 def test_multi_frame_statistics_track_oracle(method, cuda_device):
     """Chaotic trajectories diverge, so several frames are compared through
     density-error and kinetic-energy statistics (GPU harness vs CPU oracle
