@@ -340,6 +340,56 @@ def time_batched(kind, dev, flush, frames=2, warm=1):
     return rec
 
 
+# ------------------------------------------------------- APIC separation ----
+def time_separation(dev, flush, reps=20, cpu_reps=2):
+    """SolverAPIC's particle-separation pass (solver_apic.py:1003-1064, the
+    reference defaults: 2 iterations, strength 0.55, rest distance 2 x the
+    particle radius, wall margin = radius) on make_scene(400000)'s column in
+    the dam-break tank, its lattice jittered by U(-0.2, 0.2) spacing (seed
+    11) so that neighbours sit inside the rest distance.  Device time per
+    call (CUDA events, L2 flushed between calls, each call from the same
+    input) against the oracle restatement on the host cores."""
+    import torch
+    import oracle
+    from fluid_simulation_b200.apic import ParticleSeparation
+    from fluid_simulation_b200.newton_shim import model_from_arrays
+    from fluid_simulation_b200.scene import make_scene
+    s = make_scene(400000)
+    rng = np.random.default_rng(11)
+    x = (s.positions + rng.uniform(-0.2, 0.2, s.positions.shape) * s.spacing).astype(np.float32)
+    m = model_from_arrays(x, np.zeros_like(x), s.mass, device=dev, radius=s.radius)
+    sep = ParticleSeparation(m, ParticleSeparation.Config(bound_lo=s.spec.bound_lo, bound_hi=s.spec.bound_hi))
+    st = m.state()
+    x0 = st.particle_q.clone()
+    times = []
+    for r in range(reps + 3):
+        st.particle_q.copy_(x0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sep.apply(st)
+        e1.record()
+        flush.zero_()
+        e1.synchronize()
+        if r >= 3:
+            times.append(e0.elapsed_time(e1))
+    xg = st.particle_q.cpu().numpy()
+    p = sep.parameters()
+    cores = oracle.num_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    for _ in range(cpu_reps):
+        xo, _ = oracle.apic_separation(x, m.particle_flags.cpu().numpy(), p, "f32")
+    t_cpu = (time.perf_counter() - t0) / cpu_reps * 1e3
+    ms = float(np.median(times))
+    n, it = s.count, p["iterations"]
+    rec = dict(workload="apic_separation_401856", particles=n, iterations=it, rest_dist=p["rest_dist"],
+               grid_dims=list(p["dims"]), value=round(n * it / (ms * 1e-3), 1), unit="particle-separations/s",
+               ms_per_call=round(ms, 4), cpu_oracle=dict(ms_per_call=round(t_cpu, 2), cores=cores),
+               speedup_vs_cpu=round(t_cpu / ms, 1), bit_identical_to_oracle=bool(np.array_equal(xg, xo)))
+    del sep, m, st
+    torch.cuda.empty_cache()
+    return rec
+
+
 # ------------------------------------------------------------- metrics ----
 def time_metrics(dev, reps=20):
     """The harness's per-frame metrics (simulation.py:198-225) on the WCSPH
@@ -602,6 +652,8 @@ def run_ours(args):
                    time_frame_loop(dev, flush, frames=3, method="dfsph")]
         elif args.only == "metrics":
             rec = time_metrics(dev)
+        elif args.only == "separation":
+            rec = time_separation(dev, flush)
         else:
             rec = time_batched(args.only.split("_")[1], dev, flush, frames=1, warm=1)
         print(json.dumps(dict(only=args.only, record=rec)), flush=True)
@@ -762,6 +814,7 @@ def run_ours(args):
         secondary["wcsph_dam_frames_50232"] = time_frame_loop(dev, flush, target=50000, frames=3)
         secondary["dfsph_dam_frames_401856"] = time_frame_loop(dev, flush, frames=3, method="dfsph")
         secondary["metrics_wcsph_dam_401856"] = time_metrics(dev)
+        secondary["apic_separation_401856"] = time_separation(dev, flush)
     if world == 1 and not args.no_secondary and not args.no_adjoint:
         secondary["adjoint_wcsph_50232"] = time_adjoint(dev, flush)
         secondary["batched_adjoint_wcsph_256"] = time_adjoint(dev, flush, batched=True)
@@ -843,7 +896,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "batched_dfsph", "frames", "metrics"],
+    ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "batched_dfsph", "frames", "metrics", "separation"],
                     help="run one secondary workload alone (profiling); no bench line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

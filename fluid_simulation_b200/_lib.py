@@ -87,6 +87,11 @@ class PbfParams(C.Structure):
         (k, F) for k in ("lambda_epsilon", "scorr_k", "scorr_n", "scorr_w_delta_q", "max_delta_position", "xsph_c")]
 
 
+class SeparationParams(C.Structure):
+    _fields_ = [("rest_dist", F), ("query_radius", F), ("strength", F), ("bound_lo", F * 3), ("bound_hi", F * 3),
+                ("wall_band", F), ("wall_margin", F), ("iterations", I32)]
+
+
 class DfsphInfo(C.Structure):
     _fields_ = [("rho_iterations", I32), ("vel_iterations", I32), ("density_residual", C.c_double),
                 ("divergence_residual", C.c_double)]
@@ -124,6 +129,7 @@ SIGNATURES = {
                                    C.POINTER(DfsphParams), P, P]),
     "fs_dfsph_info_read": (C.c_int, [P, C.POINTER(DfsphInfo)]),
     "fs_dfsph_info_worlds": (C.c_int, [P, C.POINTER(DfsphInfo), C.c_int32]),
+    "fs_apic_separation": (C.c_int, [P, P, P, C.c_int64, C.POINTER(SeparationParams), P, P]),
     "fs_pbf_substep": (C.c_int, [P, C.POINTER(Model), C.POINTER(State), C.POINTER(State),
                                  C.POINTER(PbfParams), P, P, P]),
     "fs_wcsph_density": (C.c_int, [P, C.POINTER(Model), P, F, I32, P, P, P]),

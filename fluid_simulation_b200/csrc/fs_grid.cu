@@ -567,7 +567,7 @@ static const char* kPassNames[P_COUNT] = {
     "grid_build", "gather", "wcsph_density", "wcsph_force", "dfsph_density_factor", "dfsph_accel", "dfsph_rate",
     "dfsph_correct", "dfsph_integrate", "dfsph_final", "pbf_predict", "pbf_density", "pbf_accel", "pbf_lambda",
     "pbf_delta", "pbf_velocity", "pbf_xsph", "wcsph_adjoint_integrate", "wcsph_adjoint_force",
-    "wcsph_adjoint_density", "other"};
+    "wcsph_adjoint_density", "other", "apic_separation"};
 
 int32_t fs_pass_count(void) { return P_COUNT; }
 

@@ -38,7 +38,7 @@ struct DfsphWorld {   // batched contexts: one world's decisions in one half of 
 enum Pass {
   P_GRID = 0, P_GATHER, P_WCSPH_DENSITY, P_WCSPH_FORCE, P_DFSPH_DENSITY_FACTOR, P_DFSPH_ACCEL, P_DFSPH_RATE,
   P_DFSPH_CORRECT, P_DFSPH_INTEGRATE, P_DFSPH_FINAL, P_PBF_PREDICT, P_PBF_DENSITY, P_PBF_ACCEL, P_PBF_LAMBDA,
-  P_PBF_DELTA, P_PBF_VELOCITY, P_PBF_XSPH, P_ADJ_INTEGRATE, P_ADJ_FORCE, P_ADJ_DENSITY, P_OTHER, P_COUNT
+  P_PBF_DELTA, P_PBF_VELOCITY, P_PBF_XSPH, P_ADJ_INTEGRATE, P_ADJ_FORCE, P_ADJ_DENSITY, P_OTHER, P_APIC_SEPARATION, P_COUNT
 };
 
 struct PassTimer {

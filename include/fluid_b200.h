@@ -120,6 +120,19 @@ typedef struct {
   float lambda_epsilon, scorr_k, scorr_n, scorr_w_delta_q, max_delta_position, xsph_c;
 } fs_pbf_params;
 
+/* SolverAPIC particle separation (solver_apic.py:1003-1064): the kernel
+ * arguments of accumulate_particle_separation / apply_particle_separation_delta
+ * (193-266) and the iteration count. */
+typedef struct {
+  float rest_dist;     /* pushes act below this distance */
+  float query_radius;  /* grid cell width and query radius (max(rest_dist, 1e-5)) */
+  float strength;      /* separation_strength */
+  float bound_lo[3], bound_hi[3];
+  float wall_band;     /* into-wall push components removed within this band */
+  float wall_margin;   /* positions clamped to the bounds inset by this margin */
+  int32_t iterations;  /* separation_iterations (at least 1) */
+} fs_separation_params;
+
 /* Per-step DFSPH solver record (read back on demand; not needed to step). */
 typedef struct {
   int32_t rho_iterations;       /* density iterations entered */
@@ -232,6 +245,16 @@ int fs_dfsph_info_read(fs_context* ctx, fs_dfsph_info* info); /* synchronises th
  * over the worlds.  Synchronises the context's last stream. */
 int fs_dfsph_info_worlds(fs_context* ctx, fs_dfsph_info* info, int32_t nworlds);
 /* SolverPBF.step (solver_pbf.py:676-954).  x_pred may be NULL (solver._x_pred [n][3]). */
+/* SolverAPIC._apply_particle_separation (solver_apic.py:1003-1064): per
+ * iteration, a grid build over x with cell width query_radius, the mean push
+ * of each active particle's active neighbours closer than rest_dist (wall-band
+ * components removed), and x += push clamped to the inset bounds.  x [n][3]
+ * is updated in place; flags[n] = Model.particle_flags; delta [n][3] receives
+ * the last iteration's pushes (solver._sep_delta).  ctx: a hash-grid context
+ * with the reference's dims for this pass, max(4, ceil(extent / query_radius))
+ * per axis, and capacity >= n.  Results equal the reference's bit for bit. */
+int fs_apic_separation(fs_context* ctx, float* x, const int32_t* flags, int64_t n, const fs_separation_params* params,
+                       float* delta, fs_stream_t stream);
 int fs_pbf_substep(fs_context* ctx, const fs_model* model, const fs_state* state_in, fs_state* state_out,
                    const fs_pbf_params* params, float* accel, float* x_pred, fs_stream_t stream);
 

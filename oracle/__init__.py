@@ -24,5 +24,6 @@ from .sph import (  # noqa: F401
     wcsph_step,
     dfsph_step,
     pbf_step,
+    apic_separation,
     num_threads,
 )

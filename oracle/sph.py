@@ -89,6 +89,12 @@ class _Pbf(C.Structure):
         ("grid", GridCfg)]
 
 
+class _Separation(C.Structure):
+    _fields_ = [("rest_dist", C.c_double), ("query_radius", C.c_double), ("strength", C.c_double),
+                ("bound_lo", C.c_double * 3), ("bound_hi", C.c_double * 3), ("wall_band", C.c_double),
+                ("wall_margin", C.c_double), ("iterations", C.c_int32), ("grid", GridCfg)]
+
+
 class DfsphInfo(C.Structure):
     _fields_ = [("rho_iterations", C.c_int32), ("vel_iterations", C.c_int32),
                 ("last_density_residual", C.c_double), ("last_divergence_residual", C.c_double)]
@@ -112,6 +118,9 @@ def _load():
                     C.POINTER(DfsphInfo)]
                 getattr(lib, f"oracle_pbf_step_{prec}").argtypes = [
                     C.POINTER(_Model), C.POINTER(_State), C.POINTER(_State), C.POINTER(_Pbf), ct, P, P]
+            for prec in ("f32", "f64"):
+                getattr(lib, f"oracle_apic_separation_{prec}").argtypes = [P, P, C.c_int64,
+                                                                          C.POINTER(_Separation), P]
             _lib = lib
     return _lib
 
@@ -297,3 +306,25 @@ def pbf_step(model, state_in, cfg, dt, precision="f32", dims=(128, 128, 128), ro
     getattr(lib, f"oracle_pbf_step_{p}")(C.byref(m), C.byref(si), C.byref(so), C.byref(c), dt, _ptr(accel),
                                         _ptr(xpred))
     return out, accel, xpred
+
+
+def apic_separation(x, flags, cfg, precision="f32"):
+    """``SolverAPIC._apply_particle_separation`` (solver_apic.py:1003-1064)
+    with the two kernels of lines 193-266: ``cfg`` holds rest_dist,
+    query_radius, strength, iterations, bound_lo, bound_hi, wall_band,
+    wall_margin and the hash-grid dims.  Returns (positions after the last
+    iteration, that iteration's pushes)."""
+    lib = _load()
+    dt_np, p = _dtype(precision)
+    xo = np.ascontiguousarray(np.asarray(x, dt_np)).copy()
+    fl = np.ascontiguousarray(np.asarray(flags, np.int32))
+    n = len(xo)
+    delta = np.zeros((n, 3), dt_np)
+    c = _Separation(rest_dist=float(cfg["rest_dist"]), query_radius=float(cfg["query_radius"]),
+                    strength=float(cfg["strength"]), wall_band=float(cfg["wall_band"]),
+                    wall_margin=float(cfg["wall_margin"]), iterations=int(cfg["iterations"]),
+                    grid=_grid_cfg(cfg["dims"], 0))
+    c.bound_lo[:] = [float(v) for v in cfg["bound_lo"]]
+    c.bound_hi[:] = [float(v) for v in cfg["bound_hi"]]
+    getattr(lib, f"oracle_apic_separation_{p}")(_ptr(xo), _ptr(fl), n, C.byref(c), _ptr(delta))
+    return xo, delta

@@ -5,6 +5,8 @@
 //   solver/sph/solver_wcsph.py  (WCSPH, lines 21-305 and step 431-535)
 //   solver/sph/solver_dfsph.py  (DFSPH, lines 24-442 and step 574-898)
 //   solver/pbf/solver_pbf.py    (PBF,   lines 24-517 and step 671-954)
+//   solver/apic/solver_apic.py  (particle separation, lines 193-266 and
+//                                _apply_particle_separation 1003-1064)
 // and the third-party neighbour search those solvers call, warp-lang 1.17.0
 // `wp.HashGrid` (not vendored by the reference; its published algorithm is
 // restated in `Grid` below).  Only tests, the smoke check and the CPU-baseline
@@ -297,6 +299,14 @@ typedef struct {
   double bound_width, bound_height, bound_length, boundary_damping, boundary_epsilon;
   GridCfg grid;
 } OraclePbfCfg;
+
+typedef struct {
+  double rest_dist, query_radius, strength;
+  double bound_lo[3], bound_hi[3];
+  double wall_band, wall_margin;
+  int32_t iterations;
+  GridCfg grid;
+} OracleSeparationCfg;
 
 typedef struct {
   int32_t rho_iterations;   // density iterations entered (kernels launched for d_rho_dt)
@@ -871,6 +881,71 @@ void pbf_step(const OracleModel& om, const OracleState& si, OracleState& so, con
   if (x_pred_out) std::memcpy(x_pred_out, xpred.data(), sizeof(T) * 3 * m.n);
 }
 
+// SolverAPIC._apply_particle_separation (solver_apic.py:1003-1064): per
+// iteration a hash grid of cell width query_radius over the current
+// positions, accumulate_particle_separation (193-248: mean push of the
+// active neighbours closer than rest_dist, components into a wall band
+// removed) and apply_particle_separation_delta (251-266: add, clamp to the
+// bounds inset by wall_margin).  x is updated in place; delta keeps the last
+// iteration's pushes.
+template <class T>
+inline T warp_max(T a, T b) { return a > b ? a : b; }
+template <class T>
+inline T warp_min(T a, T b) { return a < b ? a : b; }
+
+template <class T>
+void apic_separation(T* x, const int32_t* flags, int64_t n, const OracleSeparationCfg& c, T* delta) {
+  const T rest = T(c.rest_dist), qr = T(c.query_radius), strength = T(c.strength), band = T(c.wall_band);
+  const T margin = T(c.wall_margin);
+  const V3<T> lo = mk(T(c.bound_lo[0]), T(c.bound_lo[1]), T(c.bound_lo[2]));
+  const V3<T> hi = mk(T(c.bound_hi[0]), T(c.bound_hi[1]), T(c.bound_hi[2]));
+  const int iters = c.iterations > 1 ? c.iterations : 1;
+  Grid<T> g;
+  for (int it = 0; it < iters; ++it) {
+    g.build(x, n, qr, c.grid);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      if (!active(flags[i])) {
+        st(delta, i, mk(T(0), T(0), T(0)));
+        continue;
+      }
+      const V3<T> xi = ld(x, i);
+      V3<T> disp = mk(T(0), T(0), T(0));
+      T count = T(0);
+      g.query(xi, qr, [&](int32_t j) {
+        if (j != i && active(flags[j])) {
+          const V3<T> rij = xi - ld(x, j);
+          const T d = length(rij);
+          if (d > T(1.0e-8) && d < rest) {
+            const V3<T> nrm = rij / d;
+            disp = disp + nrm * (strength * (rest - d));
+            count = count + T(1);
+          }
+        }
+      });
+      if (count > T(0))
+        disp = disp / count;
+      else
+        disp = mk(T(0), T(0), T(0));
+      if (xi.x <= lo.x + band && disp.x < T(0)) disp.x = T(0);
+      if (xi.x >= hi.x - band && disp.x > T(0)) disp.x = T(0);
+      if (xi.y <= lo.y + band && disp.y < T(0)) disp.y = T(0);
+      if (xi.y >= hi.y - band && disp.y > T(0)) disp.y = T(0);
+      if (xi.z <= lo.z + band && disp.z < T(0)) disp.z = T(0);
+      if (xi.z >= hi.z - band && disp.z > T(0)) disp.z = T(0);
+      st(delta, i, disp);
+    }
+    const V3<T> blo = lo + mk(margin, margin, margin), bhi = hi - mk(margin, margin, margin);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      if (!active(flags[i])) continue;
+      const V3<T> p = ld(x, i) + ld(delta, i);
+      st(x, i, mk(warp_min(warp_max(p.x, blo.x), bhi.x), warp_min(warp_max(p.y, blo.y), bhi.y),
+                  warp_min(warp_max(p.z, blo.z), bhi.z)));
+    }
+  }
+}
+
 }  // namespace
 
 // ----------------------------------------------------------- C entries ----
@@ -948,6 +1023,17 @@ int oracle_pbf_step_f32(const OracleModel* m, const OracleState* si, OracleState
 int oracle_pbf_step_f64(const OracleModel* m, const OracleState* si, OracleState* so, const OraclePbfCfg* c,
                         double dt, double* accel, double* x_pred) {
   pbf_step<double>(*m, *si, *so, *c, dt, accel, x_pred);
+  return 0;
+}
+
+int oracle_apic_separation_f32(float* x, const int32_t* flags, int64_t n, const OracleSeparationCfg* c, float* delta) {
+  apic_separation<float>(x, flags, n, *c, delta);
+  return 0;
+}
+
+int oracle_apic_separation_f64(double* x, const int32_t* flags, int64_t n, const OracleSeparationCfg* c,
+                               double* delta) {
+  apic_separation<double>(x, flags, n, *c, delta);
   return 0;
 }
 

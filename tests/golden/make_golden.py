@@ -6,7 +6,9 @@ Run once in a container that holds the reference sources:
 
 It executes the UNMODIFIED reference solvers (``solver/sph/solver_wcsph.py``,
 ``solver/sph/solver_dfsph.py``, ``solver/pbf/solver_pbf.py``) through their
-public ``step(state_in, state_out, control, contacts, dt)`` under the
+public ``step(state_in, state_out, control, contacts, dt)``, and the APIC
+solver's particle-separation kernels (``solver/apic/solver_apic.py``) through
+the loop of ``_apply_particle_separation``, under the
 substitute Warp/Newton runtime of ``warp_shim.py`` (FP32, one Python call per
 thread), and the reference scene generator ``examples/dam_break/scene.py``.
 Each case is saved as ``<case>.npz`` holding the inputs, the config (JSON)
@@ -98,6 +100,79 @@ def make_state(wp, sc, names_vec, names_scalar, names_int, init=None):
         setattr(sph, k, wp.array(np.zeros((n, 3), np.float32), dtype=wp.vec3))
     return _ns(particle_q=wp.array(sc["x"], dtype=wp.vec3), particle_qd=wp.array(sc["v"], dtype=wp.vec3),
                body_count=0, joint_q=None, joint_qd=None, sph=sph)
+
+
+def apic_separation_kernels(wp, newton, reference):
+    """The two particle-separation kernels of solver/apic/solver_apic.py
+    (accumulate_particle_separation, apply_particle_separation_delta, lines
+    193-266), compiled from the reference source on their own: the module
+    itself needs warp.fem and warp.sparse, which the shim does not provide."""
+    import ast
+    path = os.path.join(reference, "solver", "apic", "solver_apic.py")
+    src = open(path).read()
+    tree = ast.parse(src)
+    keep = [node for node in tree.body if isinstance(node, ast.FunctionDef)
+            and node.name in ("accumulate_particle_separation", "apply_particle_separation_delta")]
+    assert len(keep) == 2
+    ns = dict(wp=wp, ParticleFlags=newton.ParticleFlags)
+    exec(compile(ast.Module(body=keep, type_ignores=[]), path, "exec"), ns)
+    return ns["accumulate_particle_separation"], ns["apply_particle_separation_delta"]
+
+
+def run_apic_separation(wp, newton, reference, name, x, flags, radius, bound_lo, bound_hi, strength=0.55,
+                        iterations=2, rest_dist_cfg=-1.0, wall_margin_cfg=-1.0, wall_push_band_cfg=-1.0):
+    """SolverAPIC._apply_particle_separation (solver_apic.py:1003-1064) with
+    the parameter derivation of SolverAPIC.__init__ (641-650) for a model of
+    uniform particle radius."""
+    accumulate, apply_delta = apic_separation_kernels(wp, newton, reference)
+    n = len(x)
+    radii = np.full(n, radius, np.float32)
+    wall_margin = float(np.mean(radii)) if wall_margin_cfg < 0.0 else float(wall_margin_cfg)
+    wall_push_band = 1.5 * wall_margin if wall_push_band_cfg < 0.0 else float(wall_push_band_cfg)
+    rest_dist = float(rest_dist_cfg) if rest_dist_cfg > 0.0 else float(2.0 * float(np.mean(radii)))
+    query_radius = max(rest_dist, 1.0e-5)
+    lo = np.asarray(bound_lo, dtype=np.float64)
+    hi = np.asarray(bound_hi, dtype=np.float64)
+    extent = np.maximum(hi - lo, query_radius)
+    dims = np.maximum(4, np.ceil(extent / query_radius).astype(int))
+    grid = wp.HashGrid(int(dims[0]), int(dims[1]), int(dims[2]))
+    pos = wp.array(x, dtype=wp.vec3)
+    fl = wp.array(flags, dtype=wp.int32)
+    delta = wp.array(np.zeros((n, 3), np.float32), dtype=wp.vec3)
+    blo, bhi = wp.vec3(*bound_lo), wp.vec3(*bound_hi)
+    band = max(float(wall_push_band), float(wall_margin) * 2.0)
+    t0 = time.time()
+    for _ in range(max(1, int(iterations))):
+        grid.build(points=pos, radius=query_radius)
+        wp.launch(kernel=accumulate, dim=n, inputs=[grid.id, pos, fl, delta, rest_dist, query_radius, strength,
+                                                     blo, bhi, band])
+        wp.launch(kernel=apply_delta, dim=n, inputs=[pos, fl, delta, blo, bhi, float(wall_margin)])
+    cfg = dict(rest_dist=rest_dist, query_radius=query_radius, strength=strength, iterations=int(iterations),
+               bound_lo=list(map(float, bound_lo)), bound_hi=list(map(float, bound_hi)), wall_band=band,
+               wall_margin=wall_margin, dims=[int(d) for d in dims], radius=float(radius))
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), in_x=x, flags=flags, config=json.dumps(cfg),
+                        out_x=pos.numpy(), out_delta=delta.numpy())
+    print(f"{name}: n={n} {time.time() - t0:.1f}s", flush=True)
+
+
+def apic_block(seed=3):
+    """Clumped jittered lattice (spacing 0.8 of the rest distance) in a small
+    tank, with particles inside the wall bands, outside the tank (their cells
+    alias through the grid's modulo), inactive ones and a coincident pair."""
+    rng = np.random.default_rng(seed)
+    r = 0.005
+    g = np.arange(9, dtype=np.float64) * 0.8 * (2 * r)
+    xx, yy, zz = np.meshgrid(g - 0.032, g - 0.032, g + 0.001, indexing="ij")
+    x = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1)
+    x += rng.uniform(-0.15, 0.15, x.shape) * r
+    out = rng.uniform([0.20, -0.03, 0.0], [0.22, 0.03, 0.06], (24, 3))     # beyond x = hi: aliased cells
+    x = np.concatenate([x, out]).astype(np.float32)
+    x[7] = x[6]                                                              # coincident pair
+    n = len(x)
+    flags = np.ones(n, np.int32)
+    flags[[3, 40, 41, 300]] = 0
+    flags[[12]] = 5
+    return x, flags, r
 
 
 def run_case(wp, name, solver_cls, cfg, sc, material, dt, state_names, init=None):
@@ -234,6 +309,11 @@ def main():
         cfg = SolverPBF.PbfConfig(max_iterations=4, lambda_epsilon=100.0, min_neighbors_for_lambda=8, scorr_k=0.0,
                                   max_delta_position=dam["radius"] * 0.5, xsph_c=0.05, **dam_common)
         run_case(wp, "pbf_dam512", SolverPBF, cfg, dam, mat, 1.0 / 240.0, pnames)
+
+    if want("apic_separation"):
+        x, flags, r = apic_block()
+        run_apic_separation(wp, newton, args.reference, "apic_separation", x, flags, r,
+                            bound_lo=(-0.05, -0.05, 0.0), bound_hi=(0.05, 0.05, 0.1))
 
     if want("scenes"):
         scenes = {}

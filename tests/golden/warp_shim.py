@@ -4,8 +4,9 @@ source on the CPU, one Python call per thread, in FP32.
 Used only by ``make_golden.py`` (fixture generation in a container that has
 the reference sources); nothing at test time imports it.  warp-lang 1.17.0 and
 newton 1.6.0 are not installable here, so this module provides the subset of
-their API that ``solver/sph/solver_wcsph.py``, ``solver/sph/solver_dfsph.py``
-and ``solver/pbf/solver_pbf.py`` use:
+their API that ``solver/sph/solver_wcsph.py``, ``solver/sph/solver_dfsph.py``,
+``solver/pbf/solver_pbf.py`` and the particle-separation kernels of
+``solver/apic/solver_apic.py`` use:
 
 * ``@wp.kernel`` / ``@wp.func`` keep the Python function; ``wp.launch`` runs
   the kernel body for tid = 0..dim-1, converting scalar arguments to the
@@ -100,6 +101,12 @@ def length(a):
 
 def _num(x):
     return isinstance(x, (float, np.floating))
+
+
+def clamp(x, a, b):
+    """warp's clamp: x limited to [a, b] (min(max(x, a), b); the ranges used
+    here all have a <= b)."""
+    return min(max(x, a), b)
 
 
 def max(a, b):  # noqa: A001 - warp name
