@@ -48,12 +48,18 @@ __global__ void k_sep_accumulate(SepArgs a) {
     return;
   }
   float dx_ = 0.f, dy_ = 0.f, dz_ = 0.f, count = 0.f;
+  // d2 above rest^2 (1 + 1e-6) gives a rounded sqrt(d2) >= rest (at least
+  // ~3 ulps above it), which the test d < rest rejects: only the remaining
+  // candidates pay for the correctly rounded square root
+  const float r2lim = __fmul_rn(__fmul_rn(a.rest, a.rest), 1.000001f);
   for_each_range(a.g, 0, xi.x, xi.y, xi.z, a.qr, [&](int b, int e) {
     for (int t = b; t < e; ++t) {
       const float4 xj = __ldg(a.xs + t);
       if (t == (int)s || !(pf_of(xj) & PF_ACTIVE)) continue;
       const float rx = __fsub_rn(xi.x, xj.x), ry = __fsub_rn(xi.y, xj.y), rz = __fsub_rn(xi.z, xj.z);
-      const float d = __fsqrt_rn(dist2_rn(rx, ry, rz));
+      const float d2 = dist2_rn(rx, ry, rz);
+      if (!(d2 <= r2lim)) continue;
+      const float d = __fsqrt_rn(d2);
       if (d > 1.0e-8f && d < a.rest) {
         const float w = __fmul_rn(a.strength, __fsub_rn(a.rest, d));
         dx_ = __fadd_rn(dx_, __fmul_rn(__fdiv_rn(rx, d), w));
