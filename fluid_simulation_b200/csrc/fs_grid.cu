@@ -26,6 +26,21 @@ constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096 cells per block
 
+// A thread's kScanItems consecutive counts: two 16-byte loads when all lie
+// below m (base is a multiple of 8, the arrays come from cudaMalloc).
+__device__ __forceinline__ void load_items(const int32_t* __restrict__ in, int64_t base, int64_t m,
+                                           int32_t (&v)[kScanItems]) {
+  static_assert(kScanItems == 8, "two int4 per thread");
+  if (base + kScanItems <= m) {
+    const int4 a = __ldg(reinterpret_cast<const int4*>(in + base));
+    const int4 b = __ldg(reinterpret_cast<const int4*>(in + base) + 1);
+    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) v[k] = base + k < m ? in[base + k] : 0;
+  }
+}
+
 __global__ void k_cell_keys(int64_t n, const float* __restrict__ x, float inv, int dim_x, int dim_y, int dim_z,
                             int rounding, int32_t* __restrict__ key, int32_t* __restrict__ slot,
                             int32_t* __restrict__ count, uint32_t* status, const fs_frame_clock* clock) {
@@ -66,12 +81,11 @@ __global__ void k_scan_reduce(const int32_t* __restrict__ in, int64_t m, int32_t
   if (clock_idle(clock)) return;
   __shared__ int32_t warp_sums[kScanThreads / 32];
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int32_t v[kScanItems];
+  load_items(in, base, m, v);
   int32_t s = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    const int64_t j = base + k;
-    if (j < m) s += in[j];
-  }
+  for (int k = 0; k < kScanItems; ++k) s += v[k];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = s;
   __syncthreads();
@@ -139,19 +153,24 @@ __global__ void k_scan_down(const int32_t* __restrict__ in, int64_t m, const int
   if (clock_idle(clock)) return;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   int32_t v[kScanItems];
+  load_items(in, base, m, v);
   int32_t s = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    const int64_t j = base + k;
-    v[k] = j < m ? in[j] : 0;
-    s += v[k];
-  }
+  for (int k = 0; k < kScanItems; ++k) s += v[k];
   int32_t run = block_exclusive_scan(s, nullptr) + part[blockIdx.x];
+  int32_t o[kScanItems];
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    const int64_t j = base + k;
-    if (j < m) out[j] = run;
+    o[k] = run;
     run += v[k];
+  }
+  if (base + kScanItems <= m) {  // two 16-byte stores
+    reinterpret_cast<int4*>(out + base)[0] = make_int4(o[0], o[1], o[2], o[3]);
+    reinterpret_cast<int4*>(out + base)[1] = make_int4(o[4], o[5], o[6], o[7]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+      if (base + k < m) out[base + k] = o[k];
   }
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[m] = part[gridDim.x];
 }
