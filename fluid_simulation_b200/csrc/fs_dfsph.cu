@@ -221,12 +221,28 @@ __device__ void residual_finish(DfsphDev* ctrl, const double* part, const int64_
   // fixed-order sum over block partials: deterministic
   __shared__ double sd[kBlock / 32];
   __shared__ long long sc[kBlock / 32];
-  double v = 0.0;
-  long long c = 0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    v += __ldcg(part + b);
-    c += __ldcg((const long long*)cntp + b);
+  // four partial sums per thread keep four loads in flight; they combine in
+  // a fixed order, so the result does not depend on timing
+  const int step = (int)blockDim.x;
+  double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+  long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+  int b = threadIdx.x;
+  for (; b + 3 * step < nblk; b += 4 * step) {
+    v0 += __ldcg(part + b);
+    v1 += __ldcg(part + b + step);
+    v2 += __ldcg(part + b + 2 * step);
+    v3 += __ldcg(part + b + 3 * step);
+    c0 += __ldcg((const long long*)cntp + b);
+    c1 += __ldcg((const long long*)cntp + b + step);
+    c2 += __ldcg((const long long*)cntp + b + 2 * step);
+    c3 += __ldcg((const long long*)cntp + b + 3 * step);
   }
+  for (; b < nblk; b += step) {
+    v0 += __ldcg(part + b);
+    c0 += __ldcg((const long long*)cntp + b);
+  }
+  double v = (v0 + v1) + (v2 + v3);
+  long long c = (c0 + c1) + (c2 + c3);
   for (int o = 16; o > 0; o >>= 1) {
     v += __shfl_down_sync(0xffffffffu, v, o);
     c += __shfl_down_sync(0xffffffffu, c, o);
