@@ -6,7 +6,8 @@
 //   off[c]       first slot of cell c; off[c+1] one past its last slot
 // Algorithm (O(N) + O(cells) HBM traffic, deterministic):
 //   1. keys:    cell key per particle, arrival slot by atomicAdd on the cell count
-//   2. scan:    exclusive prefix of the counts (three-phase block scan)
+//   2. scan:    exclusive prefix of the counts (tile sums, then a down-sweep
+//               in which each tile adds up the sums before it)
 //   3. scatter: tmp[off[key] + arrival] = i        (order inside a cell arbitrary)
 //   4. rank:    slot = off[key] + #{j in cell : j < i}; perm[slot] = i
 // Step 4 restores ascending original index inside each cell, which is the
@@ -125,39 +126,24 @@ __device__ int32_t block_exclusive_scan(int32_t v, int32_t* total) {
   return res;
 }
 
-// phase 2: exclusive scan of the tile sums (one block, <= 1024 * 4 tiles)
-__global__ void k_scan_partials(int32_t* part, int nb, const fs_frame_clock* clock) {
-  if (clock_idle(clock)) return;
-  constexpr int kItems = 4;
-  const int base = threadIdx.x * kItems;
-  int32_t v[kItems];
-  int32_t s = 0;
-#pragma unroll
-  for (int k = 0; k < kItems; ++k) {
-    v[k] = base + k < nb ? part[base + k] : 0;
-    s += v[k];
-  }
-  int32_t total = 0;
-  int32_t run = block_exclusive_scan(s, &total);
-#pragma unroll
-  for (int k = 0; k < kItems; ++k) {
-    if (base + k < nb) part[base + k] = run;
-    run += v[k];
-  }
-  if (threadIdx.x == 0) part[nb] = total;
-}
-
-// phase 3: scan inside tiles, offset by the tile prefix; out has m + 1 entries
+// phase 2: scan inside tiles, offset by the sum of the preceding tiles
+// counts (each block adds up part[0 .. blockIdx.x) itself: at most a few
+// thousand integers, exact in any order); out has m + 1 entries
 __global__ void k_scan_down(const int32_t* __restrict__ in, int64_t m, const int32_t* __restrict__ part,
                             int32_t* __restrict__ out, const fs_frame_clock* clock) {
   if (clock_idle(clock)) return;
+  int32_t before = 0;
+  for (int k = threadIdx.x; k < (int)blockIdx.x; k += blockDim.x) before += __ldcg(part + k);
+  int32_t prefix = 0;
+  block_exclusive_scan(before, &prefix);
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   int32_t v[kScanItems];
   load_items(in, base, m, v);
   int32_t s = 0;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) s += v[k];
-  int32_t run = block_exclusive_scan(s, nullptr) + part[blockIdx.x];
+  int32_t tile = 0;
+  int32_t run = block_exclusive_scan(s, &tile) + prefix;
   int32_t o[kScanItems];
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
@@ -172,7 +158,7 @@ __global__ void k_scan_down(const int32_t* __restrict__ in, int64_t m, const int
     for (int k = 0; k < kScanItems; ++k)
       if (base + k < m) out[base + k] = o[k];
   }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[m] = part[gridDim.x];
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[m] = prefix + tile;
 }
 
 __global__ void k_scatter(int64_t n, const int32_t* __restrict__ key, const int32_t* __restrict__ slot,
@@ -267,7 +253,7 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
   if (n > c->capacity) return set_error(FS_ERR_CAPACITY, "grid_build: n=%lld > capacity=%lld", (long long)n,
                                         (long long)c->capacity);
   const float inv = 1.0f / radius;
-  PassScope ps_(c, P_GRID, st, n > 0 ? 6 : 3);
+  PassScope ps_(c, P_GRID, st, n > 0 ? 5 : 2);
   int rc = check_cuda(cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * c->ncell, st), "memset cell counts");
   if (rc) return rc;
   // a new grid invalidates recorded neighbour lists
@@ -281,7 +267,6 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
                                                    c->grid.rounding, c->key, c->slot, c->cell_count, c->status, clock);
   const int nb = scan_blocks(c->ncell);
   k_scan_reduce<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, clock);
-  k_scan_partials<<<1, 1024, 0, st>>>(c->scan_part, nb, clock);
   k_scan_down<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, c->cell_off, clock);
   if (n > 0) {
     k_scatter<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->slot, c->cell_off, c->tmp_ids, clock);
