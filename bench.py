@@ -31,6 +31,7 @@ the only published solve time (64.65 ms per 4-substep frame on an RTX 4090,
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -125,20 +126,26 @@ def build_workload(name, device):
     from fluid_simulation_b200.newton_shim import model_from_arrays
     from fluid_simulation_b200.scene import make_scene, stress_lattice
     from fluid_simulation_b200.solver import SolverDFSPH, SolverPBF, SolverWCSPH
-    if name in ("pbf_dam_401856", "dfsph_dam_401856"):
+    if name in ("pbf_dam_401856", "dfsph_dam_401856", "pbf_dam_401856_scorr"):
         kind = name.split("_")[0]
         s = make_scene(400000)
         cls = {"pbf": SolverPBF, "dfsph": SolverDFSPH}[kind]
         attrs = dict(material(kind, s), particle_mask=0)
         m = model_from_arrays(s.positions, np.zeros_like(s.positions), s.mass, device=device, radius=s.radius,
                               gravity=(s.spec.gravity,), attributes=attrs, solver_cls=cls)
-        solver = cls(m, solver_config(kind, s))
+        cfg = solver_config(kind, s)
+        if name.endswith("_scorr"):
+            # artificial pressure on, at the solver class's defaults (k = 1e-4, n = 4, q = 0.3)
+            d = SolverPBF.PbfConfig()
+            cfg = dataclasses.replace(cfg, scorr_k=d.scorr_k, scorr_n=d.scorr_n, scorr_q=d.scorr_q)
+        solver = cls(m, cfg)
         desc = dict(workload=name, particles=s.count, scene="make_scene(400000) dam break",
                     solver=kind.upper(), dt=SUBSTEP_DT[kind] if kind == "pbf" else
                     "harness CFL: min(rest of frame, 1/240, 0.4 spacing / max|v|)", spacing=s.spacing)
         if kind == "pbf":
-            desc.update(constraint_iterations=4, substeps_per_frame=4, artificial_pressure="off (harness scorr_k=0)",
-                        xsph_c=0.05)
+            desc.update(constraint_iterations=4, substeps_per_frame=4, artificial_pressure=(
+                f"on (k={cfg.scorr_k:g}, n={cfg.scorr_n:g}, q={cfg.scorr_q:g}: the solver class defaults)"
+                if cfg.scorr_k else "off (harness scorr_k=0)"), xsph_c=0.05)
         else:
             desc.update(max_rho_iterations=5, max_vel_iterations=12, warm_start=False)
         return m, solver, SUBSTEP_DT[kind], s.count, desc
@@ -178,7 +185,12 @@ def cpu_oracle_setup(name):
                  particle_world=np.zeros(n, np.int32), gravity=np.array([s.spec.gravity], np.float32),
                  particle_max_radius=s.radius, sph=sph)
     state = dict(particle_q=s.positions.copy(), particle_qd=np.zeros_like(s.positions), sph={})
-    return kind, model, state, asdict(solver_config(kind, s)), n
+    cfg = asdict(solver_config(kind, s))
+    if name.endswith("_scorr"):  # as build_workload: artificial pressure at the class defaults
+        from fluid_simulation_b200.solver import SolverPBF
+        d = SolverPBF.PbfConfig()
+        cfg.update(scorr_k=d.scorr_k, scorr_n=d.scorr_n, scorr_q=d.scorr_q)
+    return kind, model, state, cfg, n
 
 
 def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1, single_thread_seconds=8.0):
@@ -784,7 +796,7 @@ def run_ours(args):
     # ---- secondary workloads (same timing rules, fewer steps), N=1 only
     secondary = {}
     if world == 1 and not args.no_secondary:
-        for wl in ("dfsph_dam_401856", "wcsph_stress_4m"):
+        for wl in ("dfsph_dam_401856", "wcsph_stress_4m", "pbf_dam_401856_scorr"):
             if wl == args.workload:
                 continue
             m2, s2, dt2, n2, d2 = build_workload(wl, dev)
@@ -902,7 +914,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pbf_dam_401856",
-                    choices=["pbf_dam_401856", "dfsph_dam_401856", "wcsph_stress_4m", "wcsph_stress_524k"])
+                    choices=["pbf_dam_401856", "dfsph_dam_401856", "wcsph_stress_4m", "wcsph_stress_524k",
+                             "pbf_dam_401856_scorr"])
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -267,7 +267,20 @@ struct DeltaArgs {
   float4* xs_out;     // may be null (separate-pass use)
 };
 
+// x^n for a small positive integer n by repeated squaring (2 products for
+// the usual n = 4, against a general powf per pair); within 2 ulp of x^n.
+FS_DEV float pow_uint(float x, int n) {
+  float r = 1.f;
+  for (; n; n >>= 1) {
+    if (n & 1) r *= x;
+    x *= x;
+  }
+  return r;
+}
+
 __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
+  // an integral exponent 1..8 (the class default is 4) takes pow_uint
+  const int n_int = (a.scorr_n >= 1.f && a.scorr_n <= 8.f && a.scorr_n == rintf(a.scorr_n)) ? (int)a.scorr_n : 0;
   for_slots(a.n, [&](int64_t s) {
     const float4 xi = a.xs[s];
     const int32_t i = a.g.perm[s];
@@ -290,7 +303,10 @@ __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
       float r, rinv;
       r_and_inv(r2, r, rinv);
       float sc = 0.f;
-      if (scorr) sc = -a.scorr_k * powf(K.w_r2(r2) * inv_wdq, a.scorr_n);
+      if (scorr) {
+        const float q = K.w_r2(r2) * inv_wdq;
+        sc = -a.scorr_k * (n_int ? pow_uint(q, n_int) : powf(q, a.scorr_n));
+      }
       const float c = (li + lj.x + sc) * lj.y * K.grad_scale(r, rinv);
       dx_ = fmaf(c, dx, dx_);
       dy_ = fmaf(c, dy, dy_);

@@ -66,6 +66,18 @@ def test_pbf_dam(target, cuda_device):
 
 
 @pytest.mark.parametrize("target", [10000, 50000])
+def test_pbf_dam_artificial_pressure(target, cuda_device):
+    """The dam break with the s_corr term on, at the solver class's defaults
+    (k = 1e-4, n = 4, q = 0.3; solver_pbf.py:526-528)."""
+    s, model, state, common = dam_setup(target)
+    cfg = dict(common, max_iterations=4, lambda_epsilon=100.0, min_neighbors_for_lambda=8, scorr_k=1.0e-4,
+               scorr_n=4.0, scorr_q=0.3, max_delta_position=s.radius * 0.5, xsph_c=0.05)
+    dt = 1.0 / 240.0
+    out, _, _ = run_step("pbf", model, state, cfg, dt)
+    compare("pbf", out, model, state, cfg, dt)
+
+
+@pytest.mark.parametrize("target", [10000, 50000])
 def test_dfsph_dam(target, cuda_device):
     s, model, state, common = dam_setup(target)
     cfg = dict(common, max_rho_iterations=5, max_vel_iterations=12, warm_start=False, eta_density=0.1,
