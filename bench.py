@@ -59,16 +59,19 @@ PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 40
 # DRAM bytes (read + write) per particle per launch, cold cache, from the
 # ncu capture of one PBF substep's four k_lambda launches at 401,856
 # particles (summary committed under profiles/): the first reuses the
-# density pass's lists and reads them back, 78.95 MB; the three scanning
-# ones 35.9 MB each; their mean.
-TRAFFIC_PER_PARTICLE = {"pbf_lambda": 46.47e6 / 401856}
-# Warp instructions per particle per launch from the same captures of the
-# PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 38.22 M for the
-# reusing launch and 81.69 M for each scanning one).  The neighbour passes
-# are bound by instruction issue, so the bench reports the issue rate beside
-# the HBM roofline.  Issue peak = 148 SMs x 4 schedulers x 1 warp instruction per
-# cycle at the SM clock sampled during the timed region.
-WARP_INST_PER_PARTICLE = {"pbf_lambda": 70.82e6 / 401856, "pbf_delta": 23.65e6 / 401856,
+# density pass's lists and reads them back, 79.49 MB; the three scanning
+# ones 41.2-42.6 MB; their mean.
+TRAFFIC_PER_PARTICLE = {"pbf_lambda": 51.32e6 / 401856}
+# Warp instructions per particle per launch from the ncu captures of the
+# PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 38.21 M for the
+# reusing launch and 82.35 M for each scanning one; PBF delta: the mean of
+# its four launches).  The WCSPH and DFSPH figures predate the row-offset
+# prefetch of the grid queries, which added under 1 % to the PBF scans.
+# The neighbour passes are bound by instruction issue, so the bench reports
+# the issue rate beside the HBM roofline.  Issue peak = 148 SMs x 4
+# schedulers x 1 warp instruction per cycle at the SM clock sampled during
+# the timed region.
+WARP_INST_PER_PARTICLE = {"pbf_lambda": 71.32e6 / 401856, "pbf_delta": 24.03e6 / 401856,
                           "wcsph_density": 118.60e6 / 524288, "wcsph_force": 49.16e6 / 524288,
                           "dfsph_density_factor": 91.04e6 / 401856, "dfsph_rate": 26.69e6 / 401856}
 FALLBACK_HBM_GBS = 6650.0
