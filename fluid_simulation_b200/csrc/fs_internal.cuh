@@ -398,11 +398,32 @@ template <class RF>
 FS_DEV void for_each_range_world(const GridDev& g, int w, float px, float py, float pz, float r, RF&& rf) {
   const WorldDev& W = g.worlds[world_index(w, g.nworlds)];
   const QueryBox b = query_box_world(g, W, px, py, pz, r);
-  for (int z = b.z0; z <= b.z1; ++z)
-    for (int y = b.y0; y <= b.y1; ++y) {
-      const int row = W.base + (z * W.dims[1] + y) * W.dims[0];
-      rf(__ldg(g.off + row + b.x0), __ldg(g.off + row + b.x1 + 1));
+  // the offsets of the next row load before the current row is scanned,
+  // as in for_each_range_hash
+  if (b.z0 > b.z1 || b.y0 > b.y1) return;
+  auto row_of = [&](int z, int y) { return W.base + (z * W.dims[1] + y) * W.dims[0]; };
+  int z = b.z0, y = b.y0, row = row_of(z, y);
+  int a = __ldg(g.off + row + b.x0), e = __ldg(g.off + row + b.x1 + 1);
+  while (true) {
+    int zn = z, yn = y + 1;
+    if (yn > b.y1) {
+      yn = b.y0;
+      ++zn;
     }
+    const bool more = zn <= b.z1;
+    int an = 0, en = 0;
+    if (more) {
+      row = row_of(zn, yn);
+      an = __ldg(g.off + row + b.x0);
+      en = __ldg(g.off + row + b.x1 + 1);
+    }
+    rf(a, e);
+    if (!more) break;
+    z = zn;
+    y = yn;
+    a = an;
+    e = en;
+  }
 }
 
 // Visits the candidates of warp's hash_grid_query(grid, p, r) in the same
