@@ -59,6 +59,25 @@ def test_grid_candidates_bit_exact(case, cuda_device):
     np.testing.assert_array_equal(cand.cpu().numpy(), cand_ref)
 
 
+@pytest.mark.parametrize("dims,rounding", [((128, 128, 128), 0), ((7, 5, 3), 1)])
+def test_far_queries_bit_exact(dims, rounding, cuda_device):
+    """Queries millions of cells away (and at +-3e38, whose scaled
+    coordinates overflow to infinity): cell coordinates clamp and wrap as in
+    warp's hash grid, including the per-cell walk of x runs that start below
+    the shifted range."""
+    rng = np.random.default_rng(2)
+    x = rng.uniform(-0.5, 0.5, (3000, 3)).astype(np.float32)
+    h = 0.05
+    q = np.array([[-1e7, 0, 0], [1e7, 0, 0], [0, -1e7, 0], [0, 0, 1e7], [-3e38, 0.1, 0.1], [3e38, -3e38, 0.0],
+                  [-2.0e5, 0.0, 0.0], [-5.3e4, 0.2, -0.2], [0.1, 0.1, 0.1]], np.float32)
+    off_ref, cand_ref = oracle.grid_candidates(x, h, q, h, dims, rounding)
+    g = HashGrid(*dims, device=cuda_device, rounding=rounding)
+    g.build(torch.as_tensor(x, device=cuda_device), h)
+    off, cand = g.candidates(torch.as_tensor(q, device=cuda_device), h)
+    np.testing.assert_array_equal(off.cpu().numpy(), off_ref)
+    np.testing.assert_array_equal(cand.cpu().numpy(), cand_ref)
+
+
 def test_neighbour_sets_match_brute_force(cuda_device):
     """Within-h neighbour sets from the GPU candidates equal an O(N^2) search."""
     rng = np.random.default_rng(3)
