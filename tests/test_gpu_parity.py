@@ -65,13 +65,15 @@ def test_pbf_dam(target, cuda_device):
     compare("pbf", out, model, state, cfg, dt)
 
 
-@pytest.mark.parametrize("target", [10000, 50000])
-def test_pbf_dam_artificial_pressure(target, cuda_device):
+@pytest.mark.parametrize("target,scorr_n", [(10000, 4.0), (50000, 4.0), (10000, 3.0), (10000, 2.5)])
+def test_pbf_dam_artificial_pressure(target, scorr_n, cuda_device):
     """The dam break with the s_corr term on, at the solver class's defaults
-    (k = 1e-4, n = 4, q = 0.3; solver_pbf.py:526-528)."""
+    (k = 1e-4, n = 4, q = 0.3; solver_pbf.py:526-528), and with an odd and
+    a non-integral exponent (the delta pass raises integral exponents by
+    repeated squaring, others with powf)."""
     s, model, state, common = dam_setup(target)
     cfg = dict(common, max_iterations=4, lambda_epsilon=100.0, min_neighbors_for_lambda=8, scorr_k=1.0e-4,
-               scorr_n=4.0, scorr_q=0.3, max_delta_position=s.radius * 0.5, xsph_c=0.05)
+               scorr_n=scorr_n, scorr_q=0.3, max_delta_position=s.radius * 0.5, xsph_c=0.05)
     dt = 1.0 / 240.0
     out, _, _ = run_step("pbf", model, state, cfg, dt)
     compare("pbf", out, model, state, cfg, dt)
