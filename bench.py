@@ -65,15 +65,13 @@ TRAFFIC_PER_PARTICLE = {"pbf_lambda": 51.32e6 / 401856}
 # Warp instructions per particle per launch from the ncu captures of the
 # PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 38.21 M for the
 # reusing launch and 82.35 M for each scanning one; PBF delta: the mean of
-# its four launches).  The WCSPH and DFSPH figures predate the row-offset
-# prefetch of the grid queries, which added under 1 % to the PBF scans.
-# The neighbour passes are bound by instruction issue, so the bench reports
+# its four launches).  The neighbour passes are bound by instruction issue, so the bench reports
 # the issue rate beside the HBM roofline.  Issue peak = 148 SMs x 4
 # schedulers x 1 warp instruction per cycle at the SM clock sampled during
 # the timed region.
 WARP_INST_PER_PARTICLE = {"pbf_lambda": 71.32e6 / 401856, "pbf_delta": 24.03e6 / 401856,
-                          "wcsph_density": 118.60e6 / 524288, "wcsph_force": 49.16e6 / 524288,
-                          "dfsph_density_factor": 91.04e6 / 401856, "dfsph_rate": 26.69e6 / 401856}
+                          "wcsph_density": 114.68e6 / 524288, "wcsph_force": 49.30e6 / 524288,
+                          "dfsph_density_factor": 92.02e6 / 401856, "dfsph_rate": 26.87e6 / 401856}
 FALLBACK_HBM_GBS = 6650.0
 SUBSTEP_DT = {"pbf": 1.0 / 240.0, "dfsph": 1.0 / 240.0}
 
