@@ -26,6 +26,10 @@ the only published solve time (64.65 ms per 4-substep frame on an RTX 4090,
   reference (Warp + Newton) cannot be installed or run on these hosts.
 * Multi-GPU (torchrun): every rank advances its own replica (weak scaling, no
   data-path collective); time = max over ranks.
+* secondary (N=1): the DFSPH dam break, the 4,194,304-particle WCSPH
+  lattice and the PBF dam break with s_corr on (each over the same number
+  of substeps as the headline), the 256-scene batches, device-side frame
+  loops, frame metrics, APIC particle separation and the WCSPH adjoint.
 """
 
 from __future__ import annotations
