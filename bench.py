@@ -53,9 +53,11 @@ sys.path.insert(0, ROOT)
 # the reference's pass dependencies: each per-particle array a pass uses is
 # read once, neighbour re-reads are cache hits, outputs written once; FP32,
 # vec3 = 12 B).  Per substep: PBF 728 B, WCSPH 180 B, DFSPH 328 B + 116 B per
-# density iteration + 108 B per divergence iteration.
+# density iteration + 108 B per divergence iteration.  PBF's final density
+# pass also does the velocity update (44 B), so its two density launches
+# average 28 + 44 / 2 B.
 B_ALG = {
-    "grid_build": 48, "pbf_predict": 60, "pbf_density": 28, "pbf_accel": 72, "pbf_lambda": 40, "pbf_delta": 56,
+    "grid_build": 48, "pbf_predict": 60, "pbf_density": 50, "pbf_accel": 72, "pbf_lambda": 40, "pbf_delta": 56,
     "pbf_velocity": 44, "pbf_xsph": 64, "wcsph_density": 40, "wcsph_force": 92, "dfsph_density_factor": 36,
     "dfsph_accel": 76, "dfsph_rate": 60, "dfsph_correct": 56, "dfsph_integrate": 36, "dfsph_final": 48,
 }

@@ -584,6 +584,34 @@ FS_DEV int particle_pf(const int32_t* flags, const int32_t* mask, int64_t i) {
   return (act ? PF_ACTIVE : 0) | (dyn ? PF_DYNAMIC : 0);
 }
 
+// Slot s (particle i = perm[s]) of the cell-order copies that the neighbour
+// loops read: xs = (x, flags + world), vs = (v, mass) when vs, and mv =
+// rest_density * volume with volume = mass / max(rest_density, 1e-6)
+// (compute_particle_volume, solver_wcsph.py:110-116) when mv.  A world index
+// past the model's worlds raises FS_STATUS_BOUNDS.
+FS_DEV void gather_common_slot(int64_t s, int32_t i, const fs_model& m, const float* __restrict__ x,
+                               const float* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs,
+                               float* __restrict__ mv, uint32_t* status, int nworlds) {
+  const float3 p = ld3(x, i);
+  const int pf = particle_pf(m.particle_flags, m.particle_mask, i);
+  // batched contexts carry the world in the flags word (queries stay in it)
+  const int w = (nworlds > 0 && m.particle_world) ? world_index(m.particle_world[i], nworlds) : 0;
+  xs[s] = make_float4(p.x, p.y, p.z, pack_pf(pf, w));
+  const float mass = m.particle_mass[i];
+  if (vs) {
+    const float3 u = ld3(v, i);
+    vs[s] = make_float4(u.x, u.y, u.z, mass);
+  }
+  if (mv) {
+    const float rd = m.rest_density[i];
+    mv[s] = rd * (mass / fmaxf(rd, 1.0e-6f));
+  }
+  if (m.particle_world) {
+    const int wi = m.particle_world[i];
+    if (wi >= m.n_worlds) atomicOr(status, FS_STATUS_BOUNDS);
+  }
+}
+
 // walls_of for a kernel in original particle order (world from particle_world)
 FS_DEV Walls walls_of_particle(const Walls& b, const GridDev& g, const fs_model& m, int64_t i) {
   if (!g.worlds) return b;

@@ -2,14 +2,13 @@
 //
 //   predict   v_pred = v + dt g; x_pred = x + dt v_pred; position bounds  (original order)
 //   grid build(x_pred)          -- the only build unless rebuild_grid_each_iteration
-//   gather    x_pred, v_pred, x_in, mass, flags -> cell order
+//   gather    x_pred, v_pred, x_in, mass, flags -> cell order          (one pass)
 //   density   (poly6)
 //   accel     non-pressure (PBF variant) + apply_non_pressure_prediction + bounds -> x_pred'
 //   repeat max_iterations:
 //     lambda  rho, C, lambda, neighbour count
 //     delta   dx (+ s_corr, clamp) and apply into the OTHER x_pred buffer (Jacobi)
-//   density   (final)
-//   velocity  (x_pred - x_in) / dt
+//   density   (final) + velocity (x_pred - x_in) / dt                  (fused)
 //   xsph      XSPH viscosity, copy to state_out, apply_bounds      (fused)
 // As in the reference, the candidate set of every pass after the build is the
 // one binned at build time, queried from the particle's current position.
@@ -46,22 +45,32 @@ __global__ void k_predict(int64_t n, fs_model m, GridDev g, const float* __restr
   st3(v_pred, i, u);
 }
 
-__global__ void k_gather_xin(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ x,
-                             float4* __restrict__ out) {
+// The common gather of x_pred / v_pred plus the substep's input positions
+// x_in (xin_s, for the velocity update) in one pass over the permutation.
+__global__ void k_gather_pbf(int64_t n, const int32_t* __restrict__ perm, fs_model m, const float* __restrict__ x_pred,
+                             const float* __restrict__ v_pred, const float* __restrict__ x_in, float4* __restrict__ xs,
+                             float4* __restrict__ vs, float* __restrict__ mv, float4* __restrict__ xin_s,
+                             uint32_t* status, int nworlds) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
-  const float3 p = ld3(x, perm[s]);
-  out[s] = make_float4(p.x, p.y, p.z, 0.f);
+  const int32_t i = perm[s];
+  gather_common_slot(s, i, m, x_pred, v_pred, xs, vs, mv, status, nworlds);
+  const float3 p = ld3(x_in, i);
+  xin_s[s] = make_float4(p.x, p.y, p.z, 0.f);
 }
 
 // compute_density (115-141), poly6, self included.  sc2[s] = (rho,
 // mass / max(rho, 1e-6)): the neighbour term of the viscosity and XSPH passes.
 // With `record` it records the neighbour lists that the next pass at the
-// same positions (accel, or XSPH) reuses.
+// same positions (accel, or XSPH) reuses.  With vout (the final density of a
+// substep) it also writes update_velocity_from_positions (403-416):
+// vout[s] = ((x_pred - x_in) / max(dt, 1e-8), m / max(rho, 1e-6)), v_pred
+// for non-dynamic particles.
 __global__ void FS_NB_BOUNDS_PBF k_density(GridDev g, NbrList L, int record, int64_t n,
                                                       const float4* __restrict__ xs, const float4* __restrict__ vs,
                                                       const float* __restrict__ mv, float h, float skin, float* rho,
-                                                      float2* __restrict__ sc2) {
+                                                      float2* __restrict__ sc2, const float4* __restrict__ xin = nullptr,
+                                                      float dt = 0.f, float4* __restrict__ vout = nullptr) {
   if (record) lists_recorded(L);
   for_slots(n, [&](int64_t s) {
     const float4 xi = xs[s];
@@ -90,7 +99,18 @@ __global__ void FS_NB_BOUNDS_PBF k_density(GridDev g, NbrList L, int record, int
       L.cnt[s] = 0;
     }
     rho[i] = acc;
-    sc2[s] = make_float2(acc, vs[s].w / fmaxf(acc, 1.0e-6f));
+    const float4 vi = vs[s];
+    const float wgt = vi.w / fmaxf(acc, 1.0e-6f);
+    sc2[s] = make_float2(acc, wgt);
+    if (vout) {
+      float3 u = xyz(vi);  // non-dynamic: v_pred == v_in
+      if (pf_of(xi) & PF_DYNAMIC) {
+        const float4 x0 = xin[s];
+        const float d = fmaxf(dt, 1.0e-8f);
+        u = make_float3((xi.x - x0.x) / d, (xi.y - x0.y) / d, (xi.z - x0.z) / d);
+      }
+      vout[s] = make_float4(u.x, u.y, u.z, wgt);  // .w: m / max(rho, 1e-6), XSPH's neighbour weight
+    }
   });
 }
 
@@ -330,22 +350,6 @@ __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
 }
 
 // update_velocity_from_positions (403-416), cell order; .w keeps the mass
-__global__ void k_velocity(int64_t n, const float4* __restrict__ xs, const float4* __restrict__ xin,
-                           const float4* __restrict__ vs, const float2* __restrict__ sc2, float dt,
-                           float4* __restrict__ vout) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const float4 xi = xs[s];
-  const float4 vi = vs[s];
-  float3 v = xyz(vi);  // non-dynamic: v_pred == v_in
-  if (pf_of(xi) & PF_DYNAMIC) {
-    const float4 x0 = xin[s];
-    const float d = fmaxf(dt, 1.0e-8f);
-    v = make_float3((xi.x - x0.x) / d, (xi.y - x0.y) / d, (xi.z - x0.z) / d);
-  }
-  vout[s] = make_float4(v.x, v.y, v.z, sc2[s].y);  // .w: m / max(rho, 1e-6), XSPH's neighbour weight
-}
-
 // apply_xsph_viscosity (435-463) + copy x_pred -> particle_q + apply_bounds (467-517)
 struct XsphArgs {
   GridDev g;
@@ -430,12 +434,8 @@ int gather_pbf(fs_context* c, const fs_model* m, const float* x_in, cudaStream_t
   const int64_t n = m->n;
   {
     PassScope ps_(c, P_GATHER, st);
-    k_gather_common<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, c->xo_tmp, c->vo_tmp, c->xs, c->vs, c->mv,
-                                                    c->status, c->nworlds);
-  }
-  {
-    PassScope ps_(c, P_GATHER, st);
-    k_gather_xin<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, x_in, c->vs2);
+    k_gather_pbf<<<blocks_for(n), kBlock, 0, st>>>(n, c->perm, *m, c->xo_tmp, c->vo_tmp, x_in, c->xs, c->vs, c->mv,
+                                                 c->vs2, c->status, c->nworlds);
   }
   return launch_check("pbf gather");
 }
@@ -577,12 +577,10 @@ int fs_pbf_substep(fs_context* c, const fs_model* m, const fs_state* si, fs_stat
   // final density on the bounded x_pred (bounds were fused into the last apply)
   const GridDev gf = grid_view(c);
   {
+    // + update_velocity_from_positions into nxt (the other x_pred buffer)
     PassScope ps_(c, P_PBF_DENSITY, st);
-    k_density<<<nb_blocks(c, n), c->nb_block, 0, st>>>(gf, L, 1, n, cur, c->vs, c->mv, h, 0.f, so->rho, c->sc2);
-  }
-  {
-    PassScope ps_(c, P_PBF_VELOCITY, st);
-    k_velocity<<<blocks_for(n), kBlock, 0, st>>>(n, cur, c->vs2, c->vs, c->sc2, dt, nxt);
+    k_density<<<nb_blocks(c, n), c->nb_block, 0, st>>>(gf, L, 1, n, cur, c->vs, c->mv, h, 0.f, so->rho, c->sc2,
+                                                       c->vs2, dt, nxt);
   }
   XsphArgs xa;
   xa.g = gf;

@@ -21,25 +21,7 @@ __global__ void k_gather_common(int64_t n, const int32_t* __restrict__ perm, fs_
                                 float* __restrict__ mv, uint32_t* status, int nworlds) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
-  const int32_t i = perm[s];
-  const float3 p = ld3(x, i);
-  const int pf = particle_pf(m.particle_flags, m.particle_mask, i);
-  // batched contexts carry the world in the flags word (queries stay in it)
-  const int w = (nworlds > 0 && m.particle_world) ? world_index(m.particle_world[i], nworlds) : 0;
-  xs[s] = make_float4(p.x, p.y, p.z, pack_pf(pf, w));
-  const float mass = m.particle_mass[i];
-  if (vs) {
-    const float3 u = ld3(v, i);
-    vs[s] = make_float4(u.x, u.y, u.z, mass);
-  }
-  if (mv) {
-    const float rd = m.rest_density[i];
-    mv[s] = rd * (mass / fmaxf(rd, 1.0e-6f));
-  }
-  if (m.particle_world) {
-    const int w = m.particle_world[i];
-    if (w >= m.n_worlds) atomicOr(status, FS_STATUS_BOUNDS);
-  }
+  gather_common_slot(s, perm[s], m, x, v, xs, vs, mv, status, nworlds);
 }
 
 // ------------------------------------------------------------- density ----
