@@ -65,9 +65,9 @@ PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 40
 # DRAM bytes (read + write) per particle per launch, cold cache, from the
 # ncu capture of one PBF substep's four k_lambda launches at 401,856
 # particles (summary committed under profiles/): the first reuses the
-# density pass's lists and reads them back, 79.49 MB; the three scanning
-# ones 41.2-42.6 MB; their mean.
-TRAFFIC_PER_PARTICLE = {"pbf_lambda": 51.32e6 / 401856}
+# density pass's lists and reads them back, 81.88 MB; the three scanning
+# ones 41.1-43.0 MB; their mean.
+TRAFFIC_PER_PARTICLE = {"pbf_lambda": 51.78e6 / 401856}
 # Warp instructions per particle per launch from the ncu captures of the
 # PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 38.21 M for the
 # reusing launch and 82.35 M for each scanning one; PBF delta: the mean of
