@@ -180,9 +180,9 @@ class DamBreakSimulation:
         """simulation.py:198-225, reduced on the device (fs_frame_metrics):
         14 doubles come back instead of every particle's x, v, rho and p.
         Minima, maxima, the speed maximum and the density percentile equal
-        the numpy reductions of ``metrics_host`` exactly; the means are
-        double-precision sums (numpy sums float32 pairwise), equal to about
-        1e-7 relative."""
+        the reference's numpy reductions on host copies exactly; the means
+        are double-precision sums (numpy sums float32 pairwise), equal to
+        about 1e-7 relative."""
         s = self.state_0
         n = s.particle_q.shape[0]
         with_sph = bool(self.frame)
@@ -213,32 +213,6 @@ class DamBreakSimulation:
                 result.update(density_p99=p99,
                               density_compression_p99=max(0.0, p99 / self.scene.spec.density - 1.0),
                               pressure_min=o[12], pressure_max=o[13])
-        return result
-
-    def metrics_host(self):
-        """simulation.py:198-225 with numpy on host copies (the reference's way)."""
-        x, v = self.state_0.particle_q.cpu().numpy(), self.state_0.particle_qd.cpu().numpy()
-        finite = bool(np.isfinite(x).all() and np.isfinite(v).all())
-        if not finite:
-            raise RuntimeError(f"Non-finite particle state at frame {self.frame}")
-        result = dict(frame=self.frame, simulation_time=self.sim_time, substeps=self.last_substeps,
-                      total_substeps=self.total_substeps, finite=finite,
-                      speed_max=float(np.linalg.norm(v, axis=1).max(initial=0.0)),
-                      height_mean=float(x[:, 2].mean()), height_min=float(x[:, 2].min()),
-                      height_max=float(x[:, 2].max()))
-        if self.frame:
-            rho = self.state_0.sph.rho.cpu().numpy()
-            if not np.isfinite(rho).all():
-                raise RuntimeError("Non-finite density")
-            result.update(density_mean=float(rho.mean()), density_min=float(rho.min()), density_max=float(rho.max()))
-            if self.method == "wcsph":
-                pressure = self.state_0.sph.pressure.cpu().numpy()
-                if not np.isfinite(pressure).all():
-                    raise RuntimeError("Non-finite pressure")
-                p99 = float(np.percentile(rho, 99))
-                result.update(density_p99=p99,
-                              density_compression_p99=max(0.0, p99 / self.scene.spec.density - 1.0),
-                              pressure_min=float(pressure.min()), pressure_max=float(pressure.max()))
         return result
 
     def check_finite(self):
