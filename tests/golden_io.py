@@ -41,19 +41,47 @@ def rel_err(a, b, scale=None):
     return float(np.abs(a - b).max()) / max(s, 1e-30)
 
 
-def compare_fields(pairs, ref64, tol=1e-5):
+# Float fields formed by cancellation, whose FP32 rounding alone can exceed
+# the 1e-5 bar on ordinary inputs: EOS pressure near rest density; PBF
+# lambda and the position correction built from it, and the velocity
+# (x_pred - x_in) / dt; DFSPH kappa, kappa_v, the density-change rate and
+# the factor (1 / (|sum g|^2 + sum |g|^2) over nearly balanced gradients),
+# and the velocities the iterations correct.
+ILL_CONDITIONED = {
+    "wcsph": {"pressure"},
+    "pbf": {"pbf_lambda", "delta_p", "particle_qd", "step_displacement"},
+    "dfsph": {"kappa", "kappa_v", "d_rho_dt", "factor", "v_star", "particle_qd"},
+}
+
+
+def _log_fallback(rec):
+    """Appends one JSON line per fallback use to $FS_PARITY_LOG (if set)."""
+    path = os.environ.get("FS_PARITY_LOG")
+    if not path:
+        return
+    rec = dict(rec, test=os.environ.get("PYTEST_CURRENT_TEST", "").split(" ")[0])
+    with open(path, "a") as f:
+        f.write(json.dumps(rec) + "\n")
+
+
+def compare_fields(pairs, ref64, *, kind, tol=1e-5):
     """Parity rule of the GPU tests.  pairs: (name, candidate, reference FP32);
-    ref64: name -> the FP64 oracle's value on the same inputs.
+    ref64: name -> the FP64 oracle's value on the same inputs; kind: the
+    solver ("wcsph", "dfsph", "pbf").
 
     * integer fields (neighbor_count): identical;
-    * float fields: max|cand - ref| <= tol * max|ref|; or, for fields whose
-      own FP32 rounding exceeds that (quantities formed by cancellation:
-      EOS pressure near rest density, PBF lambda, DFSPH kappa_v, velocities
-      derived as position differences / dt, forces of nearly balanced
-      pressure), the candidate's distance from the FP64 solution is at most
-      4x the FP32 reference's own distance from it, or tol * max|FP64|.
-    Returns (errors, conditioned) lists of messages."""
+    * every float field: max|cand - ref| <= tol * max|ref| (norm-relative);
+    * otherwise, a field of ILL_CONDITIONED[kind] passes when the
+      candidate's distance from the FP64 solution is at most 4x the FP32
+      reference's own distance from it (or tol * max|FP64|);
+    * any other field (positions, densities, accelerations) passes that way
+      only when the FP32 reference itself misses the bar against FP64 on
+      this input (FP32 cannot meet it there), and then within 2x the FP32
+      reference's own distance from FP64.
+    Returns (errors, conditioned) lists of messages; each fallback use is
+    also appended to $FS_PARITY_LOG."""
     errors, conditioned = [], []
+    named = ILL_CONDITIONED[kind]
     for name, got, ref in pairs:
         got = np.asarray(got)
         ref = np.asarray(ref)
@@ -70,11 +98,22 @@ def compare_fields(pairs, ref64, tol=1e-5):
             errors.append(f"{name}: rel err {e:.3e} (no FP64 reference)")
             continue
         r64 = np.asarray(r64, np.float64)
+        scale = max(float(np.abs(r64).max()), 1e-30)
         eg = float(np.abs(got.astype(np.float64) - r64).max())
         er = float(np.abs(ref.astype(np.float64) - r64).max())
-        bound = max(tol * float(np.abs(r64).max()), 4.0 * er)
-        msg = f"{name}: rel err {e:.3e} vs FP32; |cand-FP64| {eg:.3e}, |FP32-FP64| {er:.3e}"
-        (conditioned if eg <= bound else errors).append(msg)
+        if name in named:
+            bound = max(tol * scale, 4.0 * er)
+        elif er > tol * scale:
+            bound = 2.0 * er
+        else:
+            errors.append(f"{name}: rel err {e:.3e} vs FP32 (FP32 itself within {er / scale:.2e} of FP64)")
+            continue
+        msg = (f"{name}: rel err {e:.3e} vs FP32; cand-FP64 {eg / scale:.3e}, FP32-FP64 {er / scale:.3e} "
+               f"(norm-relative)")
+        ok = eg <= bound
+        (conditioned if ok else errors).append(msg)
+        _log_fallback(dict(kind=kind, field=name, named=name in named, ok=ok, err_vs_fp32=e,
+                           cand_vs_fp64=eg / scale, fp32_vs_fp64=er / scale))
     return errors, conditioned
 
 

@@ -107,7 +107,7 @@ def test_wcsph_half_cells_keep_parity(cuda_device):
     got = dict(particle_q=b.particle_q.cpu().numpy(), particle_qd=b.particle_qd.cpu().numpy(),
                accel=solver._particle_accel.cpu().numpy(), rho=b.sph.rho.cpu().numpy(),
                pressure=b.sph.pressure.cpu().numpy())
-    errors, _ = compare_fields([(k, got[k], v) for k, v in ref32.items()], ref64)
+    errors, _ = compare_fields([(k, got[k], v) for k, v in ref32.items()], ref64, kind="wcsph")
     assert not errors, errors
 
 

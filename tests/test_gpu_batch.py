@@ -164,7 +164,7 @@ def test_batched_step_matches_oracle_per_scene(kind, cuda_device):
         ref64 = oracle_outputs(kind, model, state, c, dt, "f64")
         cnt = ref32.pop("neighbor_count", None)
         pairs = [(name, got[name][sl], val) for name, val in ref32.items()]
-        errors, _ = compare_fields(pairs, ref64)
+        errors, _ = compare_fields(pairs, ref64, kind=kind)
         assert not errors, f"scene {k}: " + "; ".join(errors)
         if cnt is not None:
             # PBF counts pairs with r < h at the positions left by three Jacobi
@@ -275,7 +275,7 @@ def test_batched_dfsph_decides_per_world(cuda_device):
         ref32 = oracle_outputs("dfsph", model, state, c, dt, "f32")
         ref64 = oracle_outputs("dfsph", model, state, c, dt, "f64")
         pairs = [(name, got[name][sl], val) for name, val in ref32.items()]
-        errors, _ = compare_fields(pairs, ref64)
+        errors, _ = compare_fields(pairs, ref64, kind="dfsph")
         assert not errors, f"scene {k}: " + "; ".join(errors)
         seen.add((per_world[k]["rho_iterations"], per_world[k]["vel_iterations"]))
     assert len(seen) > 1  # the worlds stopped at different iterations

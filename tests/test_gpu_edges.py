@@ -101,7 +101,7 @@ def test_masked_particles_stay_and_push(kind, cuda_device):
     state = dict(particle_q=x, particle_qd=v, sph=dict(kappa=np.zeros(n, np.float32), kappa_v=np.zeros(n, np.float32)))
     ref32 = oracle_outputs(kind, model, state, cfg, dt, "f32")
     ref64 = oracle_outputs(kind, model, state, cfg, dt, "f64")
-    errors, _ = compare_fields([("particle_q", q, ref32["particle_q"])], ref64)
+    errors, _ = compare_fields([("particle_q", q, ref32["particle_q"])], ref64, kind=kind)
     assert not errors, errors
 
 
@@ -150,7 +150,7 @@ def test_far_positions_alias_in_the_hash_and_keep_parity(kind, cuda_device):
     ref64 = oracle_outputs(kind, model, state, asdict(solver.config), dt, "f64")
     got = dict(particle_q=b.particle_q.cpu().numpy(), particle_qd=b.particle_qd.cpu().numpy(),
                rho=b.sph.rho.cpu().numpy())
-    errors, _ = compare_fields([(k, got[k], ref32[k]) for k in got], ref64)
+    errors, _ = compare_fields([(k, got[k], ref32[k]) for k in got], ref64, kind=kind)
     assert not errors, errors
 
 

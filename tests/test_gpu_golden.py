@@ -30,7 +30,7 @@ def test_gpu_step_matches_reference(name, cuda_device):
         if k != "step_displacement":  # never written by the reference step (launch commented out)
             pairs.append((k, out["sph"][k], ref))
     ref64 = oracle_outputs(kind, model, state_in, cfg, dt, "f64")
-    errors, conditioned = compare_fields(pairs, ref64)
+    errors, conditioned = compare_fields(pairs, ref64, kind=kind)
     assert not errors, f"{name}: " + "; ".join(errors)
     if conditioned:
         print(f"{name}: conditioned fields: " + "; ".join(conditioned))

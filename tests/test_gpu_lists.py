@@ -77,7 +77,7 @@ def test_full_and_overflowing_lists_keep_parity(kind, coff, cuda_device):
     flat = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], accel=out["accel"], **out["sph"])
     if "x_pred" in out:
         flat["x_pred"] = out["x_pred"]
-    errors, _ = compare_fields([(k, flat[k], v) for k, v in ref32.items()], ref64)
+    errors, _ = compare_fields([(k, flat[k], v) for k, v in ref32.items()], ref64, kind=kind)
     assert not errors, "; ".join(errors)
     if kind == "dfsph":
         _, _, info = oracle.dfsph_step(model, state, cfg, dt)
