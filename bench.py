@@ -67,7 +67,16 @@ PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 40
 # particles (summary committed under profiles/): the first reuses the
 # density pass's lists and reads them back, 81.88 MB; the three scanning
 # ones 41.1-43.0 MB; their mean.
-TRAFFIC_PER_PARTICLE = {"pbf_lambda": 51.78e6 / 401856}
+TRAFFIC_PER_PARTICLE = {"pbf_lambda": 51.78e6 / 401856, "dfsph_rate": 68.17e6 / 401856,
+                        "dfsph_density_factor": 36.86e6 / 401856, "wcsph_density": 73.53e6 / 524288,
+                        "wcsph_force": 95.78e6 / 524288}
+TRAFFIC_SOURCE = {
+    "pbf_lambda": "ncu, mean of one substep's 4 launches at 401,856 particles (profiles/pbf_dam_401856.md)",
+    "dfsph_rate": "ncu, one launch at 401,856 particles (profiles/dfsph_dam_401856.md)",
+    "dfsph_density_factor": "ncu, one launch at 401,856 particles (profiles/dfsph_dam_401856.md)",
+    "wcsph_density": "ncu at 524,288 particles (profiles/wcsph_bcc_524k.md), scaled by the particle count",
+    "wcsph_force": "ncu at 524,288 particles (profiles/wcsph_bcc_524k.md), scaled by the particle count",
+}
 # Warp instructions per particle per launch from the ncu captures of the
 # PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 38.21 M for the
 # reusing launch and 82.35 M for each scanning one; PBF delta: the mean of
@@ -131,8 +140,9 @@ def build_workload(name, device):
     """(model, solver, dt, n, description)."""
     from fluid_simulation_b200.dam_break import material, solver_config
     from fluid_simulation_b200.newton_shim import model_from_arrays
-    from fluid_simulation_b200.scene import make_scene, stress_lattice
+    from fluid_simulation_b200.scene import make_scene
     from fluid_simulation_b200.solver import SolverDFSPH, SolverPBF, SolverWCSPH
+    desc = workload_desc(name)
     if name in ("pbf_dam_401856", "dfsph_dam_401856", "pbf_dam_401856_scorr"):
         kind = name.split("_")[0]
         s = make_scene(400000)
@@ -145,43 +155,74 @@ def build_workload(name, device):
             # artificial pressure on, at the solver class's defaults (k = 1e-4, n = 4, q = 0.3)
             d = SolverPBF.PbfConfig()
             cfg = dataclasses.replace(cfg, scorr_k=d.scorr_k, scorr_n=d.scorr_n, scorr_q=d.scorr_q)
-        solver = cls(m, cfg)
-        desc = dict(workload=name, particles=s.count, scene="make_scene(400000) dam break",
-                    solver=kind.upper(), dt=SUBSTEP_DT[kind] if kind == "pbf" else
-                    "harness CFL: min(rest of frame, 1/240, 0.4 spacing / max|v|)", spacing=s.spacing)
-        if kind == "pbf":
-            desc.update(constraint_iterations=4, substeps_per_frame=4, artificial_pressure=(
-                f"on (k={cfg.scorr_k:g}, n={cfg.scorr_n:g}, q={cfg.scorr_q:g}: the solver class defaults)"
-                if cfg.scorr_k else "off (harness scorr_k=0)"), xsph_c=0.05)
-        else:
-            desc.update(max_rho_iterations=5, max_vel_iterations=12, warm_start=False)
-        return m, solver, SUBSTEP_DT[kind], s.count, desc
+        return m, cls(m, cfg), SUBSTEP_DT[kind], s.count, desc
     if name in ("wcsph_stress_4m", "wcsph_stress_524k"):
-        # BCC: 2 * 128^3 = 4,194,304 at d = 9.92 mm; the 524k variant (2 * 64^3 in a 0.8 m cube,
-        # same spacing) is the small case of the profiling captures
-        cells, box = (128, 1.6) if name == "wcsph_stress_4m" else (64, 0.8)
-        x, v, sp = stress_lattice(cells=cells, box=box)
+        x, v, sp, half, box, dt, cells = stress_setup(name)
         m = model_from_arrays(x, v, 1000.0 * sp ** 3, device=device, radius=0.5 * sp,
                               attributes=dict(rest_density=1000.0, surface_tension=0.0, viscosity=1e-6,
                                               stiffness=2.5e5, exponent=7.0, particle_mask=0), solver_cls=SolverWCSPH)
-        half = 0.5 * box
         solver = SolverWCSPH(m, SolverWCSPH.SphConfig(particle_radius=0.5 * sp, particle_length=sp,
                                                       smoothing_length_coff=2.0, boundary_damping=0.0,
                                                       bound_width=half, bound_height=half, bound_length=half))
-        c0 = (2.5e5 * 7.0 / 1000.0) ** 0.5
-        h = 2.0 * sp
-        dt = 0.25 * h / (c0 + float(np.linalg.norm(v, axis=1).max()))
-        return m, solver, dt, len(x), dict(workload=name, particles=len(x), scene=f"jittered BCC lattice 2 x {cells}^3 "
-                                           f"filling [-{half},{half}]^2 x [0,{box}] m, v ~ N(0, 0.2)", solver="WCSPH",
-                                           dt=dt, h=h, spacing=sp)
+        return m, solver, dt, len(x), desc
     raise SystemExit(f"unknown workload {name}")
 
 
+def stress_setup(name):
+    """Lattice, spacing, tank half-width and fixed acoustic dt of a WCSPH
+    stress workload: BCC 2 x 128^3 = 4,194,304 particles at d = 9.92 mm in
+    a 1.6 m cube, or (the small case of the profiling captures) 2 x 64^3 in
+    a 0.8 m cube at the same spacing."""
+    from fluid_simulation_b200.scene import stress_lattice
+    cells, box = (128, 1.6) if name == "wcsph_stress_4m" else (64, 0.8)
+    x, v, sp = stress_lattice(cells=cells, box=box)
+    c0 = (2.5e5 * 7.0 / 1000.0) ** 0.5
+    dt = 0.25 * (2.0 * sp) / (c0 + float(np.linalg.norm(v, axis=1).max()))
+    return x, v, sp, 0.5 * box, box, dt, cells
+
+
+def workload_desc(name):
+    """The workload's description (the bench line's config), without a GPU."""
+    if name.startswith("wcsph_stress"):
+        x, v, sp, half, box, dt, cells = stress_setup(name)
+        return dict(workload=name, particles=len(x), scene=f"jittered BCC lattice 2 x {cells}^3 filling "
+                    f"[-{half},{half}]^2 x [0,{box}] m, v ~ N(0, 0.2)", solver="WCSPH", dt=dt, h=2.0 * sp,
+                    spacing=sp)
+    from fluid_simulation_b200.scene import make_scene
+    kind = name.split("_")[0]
+    s = make_scene(400000)
+    desc = dict(workload=name, particles=s.count, scene="make_scene(400000) dam break", solver=kind.upper(),
+                dt=SUBSTEP_DT[kind] if kind == "pbf" else "harness CFL: min(rest of frame, 1/240, 0.4 spacing / "
+                "max|v|)", spacing=s.spacing)
+    if kind == "pbf":
+        scorr = ("on (k=0.0001, n=4, q=0.3: the solver class defaults)" if name.endswith("_scorr")
+                 else "off (harness scorr_k=0)")
+        desc.update(constraint_iterations=4, substeps_per_frame=4, artificial_pressure=scorr, xsph_c=0.05)
+    else:
+        desc.update(max_rho_iterations=5, max_vel_iterations=12, warm_start=False)
+    return desc
+
+
 def cpu_oracle_setup(name):
-    """Oracle-form model/state/config of the same workload (numpy)."""
+    """Oracle-form model/state/config of the same workload (numpy), and its
+    substep clock."""
+    from dataclasses import asdict
+    if name.startswith("wcsph_stress"):
+        x, v, sp, half, box, dt, cells = stress_setup(name)
+        n = len(x)
+        mat = dict(rest_density=1000.0, surface_tension=0.0, viscosity=1e-6, stiffness=2.5e5, exponent=7.0)
+        sph = {k: np.full(n, val, np.float32) for k, val in mat.items()}
+        sph["particle_mask"] = np.zeros(n, np.int32)
+        model = dict(particle_flags=np.ones(n, np.int32), particle_mass=np.full(n, 1000.0 * sp ** 3, np.float32),
+                     particle_world=np.zeros(n, np.int32), gravity=np.array([[0.0, 0.0, -10.0]], np.float32),
+                     particle_max_radius=0.5 * sp, sph=sph)
+        cfg = dict(particle_radius=0.5 * sp, particle_length=sp, smoothing_length_coff=2.0, boundary_damping=0.0,
+                   bound_width=half, bound_height=half, bound_length=half, clamp_negative_pressure=True)
+        clock = HarnessClock("wcsph", sp)
+        clock.next = lambda v: dt  # fixed acoustic dt, as on the GPU
+        return "wcsph", model, dict(particle_q=x, particle_qd=v, sph={}), cfg, n, clock
     from fluid_simulation_b200.dam_break import material, solver_config
     from fluid_simulation_b200.scene import make_scene
-    from dataclasses import asdict
     kind = name.split("_")[0]
     s = make_scene(400000)
     n = s.count
@@ -197,23 +238,33 @@ def cpu_oracle_setup(name):
         from fluid_simulation_b200.solver import SolverPBF
         d = SolverPBF.PbfConfig()
         cfg.update(scorr_k=d.scorr_k, scorr_n=d.scorr_n, scorr_q=d.scorr_q)
-    return kind, model, state, cfg, n
+    return kind, model, state, cfg, n, HarnessClock(kind, cfg["particle_length"])
+
+
+def oracle_stepper(kind):
+    import oracle
+    step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step, "wcsph": oracle.wcsph_step}[kind]
+
+    def advance(model, state, cfg, dt):
+        out = step(model, state, cfg, dt)[0]
+        return dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+    return advance
 
 
 def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1, single_thread_seconds=8.0):
-    """Substeps of the CPU oracle until max_seconds have passed, on all host
-    threads; then (single_thread_seconds > 0) the same on one thread."""
+    """Substeps of the CPU oracle from the workload's initial state until
+    max_seconds have passed, on all host threads; then
+    (single_thread_seconds > 0) the same on one thread."""
     import oracle
-    kind, model, state0, cfg, n = cpu_oracle_setup(name)
-    step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step}[kind]
+    kind, model, state0, cfg, n, _ = cpu_oracle_setup(name)
+    advance = oracle_stepper(kind)
 
     def run(seconds):
-        clock = HarnessClock(kind, cfg["particle_length"])
+        clock = cpu_oracle_setup(name)[5] if kind == "wcsph" else HarnessClock(kind, cfg["particle_length"])
         state, k = state0, 0
         t0 = time.perf_counter()
         while k < max_steps and (k < min_steps or time.perf_counter() - t0 < seconds):
-            out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
-            state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+            state = advance(model, state, cfg, clock.next(state["particle_qd"]))
             k += 1
         return k, time.perf_counter() - t0
 
@@ -221,8 +272,8 @@ def time_cpu_baseline(name, max_seconds=20.0, max_steps=1000, min_steps=1, singl
     cores = oracle.num_threads(all_threads)
     k, el = run(max_seconds)
     rec = dict(value=n * k / el, unit="particle-steps/s", cores=cores, kind="port",
-               sample=f"{k} consecutive substeps of the full {n}-particle workload in {el:.1f} s "
-                      f"(C++ restatement of the reference solver, OpenMP, {cores} threads)")
+               sample=f"the first {k} consecutive substeps of the full {n}-particle workload from its initial "
+                      f"state in {el:.1f} s (C++ restatement of the reference solver, OpenMP, {cores} threads)")
     if single_thread_seconds > 0:
         oracle.num_threads(1)
         try:
@@ -432,7 +483,9 @@ def time_metrics(dev, reps=20):
         return (time.perf_counter() - t0) / k * 1e3, out
 
     t_dev, m_dev = wall(sim.metrics, reps)
-    t_host, m_host = wall(sim.metrics_host, max(3, reps // 4))
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests"))
+    from numpy_metrics import numpy_frame_metrics  # the reference's way, as a checker
+    t_host, m_host = wall(lambda: numpy_frame_metrics(sim), max(3, reps // 4))
     exact = ("speed_max", "height_min", "height_max", "density_min", "density_max", "density_p99", "pressure_min",
              "pressure_max")
     worst_mean = max(abs(m_dev[k] - m_host[k]) / max(abs(m_host[k]), 1e-30) for k in ("height_mean", "density_mean"))
@@ -452,15 +505,16 @@ def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
     substeps, segments replayed in the backward).  Loss: mean squared distance
     of the final positions to the initial ones moved by +0.3 m in x;
     gradients w.r.t. v0 [N, 3], stiffness, viscosity and rest density.
-    Workload: make_scene(50000) (50,232 particles) or, batched, the 256 scenes
-    of make_batch() as one model."""
+    Workload: make_scene(50000) (50,232 particles) with a seeded N(0, 0.1
+    m/s) initial velocity field, so that pressure and viscosity act (the
+    gradient tests' active_column), or, batched, the 256 scenes of
+    make_batch() as one model (at rest)."""
     import torch
     from fluid_simulation_b200.batch import batched_model, make_batch
     from fluid_simulation_b200.dam_break import material, solver_config
     from fluid_simulation_b200.diff import DiffWCSPH
     from fluid_simulation_b200.graph import FrameGraph
     from fluid_simulation_b200.newton_shim import model_from_arrays
-    from fluid_simulation_b200.scene import make_scene
     from fluid_simulation_b200.solver import SolverWCSPH
     if batched:
         b = make_batch()
@@ -471,15 +525,19 @@ def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
         visc = torch.as_tensor(b.per_particle("viscosity"), device=dev)
         rest = torch.full_like(stiff, 1000.0)
         desc = dict(workload="batched_adjoint_wcsph_256", scenes=len(b.scenes), particles=b.total)
+        v_init = torch.zeros_like(model.particle_q)
     else:
-        s = make_scene(50000)
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from adjoint_util import active_column  # the gradient tests' workload
+        s, _, _, x_np, v_np, dt = active_column()
         attrs = dict(material("wcsph", s), particle_mask=0)
-        model = model_from_arrays(s.positions, np.zeros_like(s.positions), s.mass, device=dev, radius=s.radius,
+        model = model_from_arrays(x_np, v_np, s.mass, device=dev, radius=s.radius,
                                   gravity=(s.spec.gravity,), attributes=attrs, solver_cls=SolverWCSPH)
         cfg = solver_config("wcsph", s)
-        dt = 0.25 * 2.0 * s.spacing / (2.5e5 * 7.0 / 1000.0) ** 0.5
         stiff, visc, rest = (torch.tensor(v, device=dev) for v in (2.5e5, 1.0e-6, 1000.0))
-        desc = dict(workload="adjoint_wcsph_50232", scene="make_scene(50000) dam break", particles=s.count)
+        v_init = torch.as_tensor(v_np, device=dev)
+        desc = dict(workload="adjoint_wcsph_50232", scene="make_scene(50000) dam-break column, v0 ~ N(0, 0.1 m/s) "
+                    "(seed 21): pressure and viscosity act, no wall contact", particles=s.count)
     n = model.particle_count
     x0 = model.particle_q.clone()
     target = x0 + torch.tensor([0.3, 0.0, 0.0], device=dev)
@@ -491,17 +549,18 @@ def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
 
     def forward_only():  # the plain substeps, all of them in one CUDA graph
         fa.particle_q.copy_(x0)
-        fa.particle_qd.zero_()
+        fa.particle_qd.copy_(v_init)
         fwd_graph.replay()
 
     def forward_eager():
         a, c = model.state(), model.state()
+        a.particle_qd.copy_(v_init)
         for _ in range(steps):
             solver.step(a, c, None, None, dt)
             a, c = c, a
 
     def fwd_bwd(which=sim):
-        leaves = [x0.clone().requires_grad_(), torch.zeros_like(x0).requires_grad_()] + \
+        leaves = [x0.clone().requires_grad_(), v_init.clone().requires_grad_()] + \
                  [t.clone().requires_grad_() for t in (stiff, visc, rest)]
         xT, _ = which.rollout(*leaves, steps)
         loss = ((xT - target) ** 2).sum(1).mean()
@@ -645,44 +704,20 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- our arm ----
-def run_ours(args):
+def measure_workload(name, dev, flush, steps, warmup, args, world=1, clocks_gpu=0, cpu_baseline=False):
+    """One workload timed the headline's way: W warm-up substeps, K timed
+    substeps (CUDA events around each, L2 flushed between them), the
+    per-pass event timer on up to 100 further substeps (dominant pass ->
+    roofline), then end to end through the solver API with host buffers.
+    Returns the record (without rank reduction for world == 1)."""
     import torch
     import torch.distributed as dist
     import ctypes as C
     from fluid_simulation_b200 import _lib
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA device")
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     lib = _lib.load()
-    if args.only:  # one secondary workload by itself (profiling); prints its record, not the bench line
-        flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        if args.only == "adjoint":
-            rec = time_adjoint(dev, flush, reps=1)
-        elif args.only == "frames":
-            rec = [time_frame_loop(dev, flush), time_frame_loop(dev, flush, target=50000, frames=3),
-                   time_frame_loop(dev, flush, frames=3, method="dfsph")]
-        elif args.only == "metrics":
-            rec = time_metrics(dev)
-        elif args.only == "separation":
-            rec = time_separation(dev, flush)
-        else:
-            rec = time_batched(args.only.split("_")[1], dev, flush, frames=1, warm=1)
-        print(json.dumps(dict(only=args.only, record=rec)), flush=True)
-        return
-
-    model, solver, dt, n, desc = build_workload(args.workload, dev)
+    model, solver, dt, n, desc = build_workload(name, dev)
     ctx = model.particle_grid._ctx
     a, b = model.state(), model.state()
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-
     clock = HarnessClock(desc["solver"].lower(), desc.get("spacing", 0.0))
     if desc["solver"] == "WCSPH":
         clock.next = lambda v: dt  # the stress lattice runs at its fixed acoustic dt
@@ -696,18 +731,18 @@ def run_ours(args):
         solver.step(a, b, None, None, dt_k)
         a, b = b, a
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step(clock.next(a.particle_qd))
     torch.cuda.synchronize()
 
-    K = args.steps
+    K = steps
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     npass = lib.fs_pass_count()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
+    sampler = ClockSampler(clocks_gpu)
+    sampler.start()
     time.sleep(0.3)
     launches0 = lib.fs_launch_count(ctx)
     for k in range(K):
@@ -720,13 +755,14 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     launches = lib.fs_launch_count(ctx) - launches0
-    clk = clocks.stop()
+    clk = sampler.stop()
     step_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    iterations = solver.last_iterations() if hasattr(solver, "last_iterations") else None
     # per-pass breakdown: further steps with the per-pass event timer on,
     # outside the timed loop (its event records would sit between the passes)
     Kp = min(K, 100)
     evp = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(Kp)]
-    _lib.check(lib.fs_timer_enable(ctx, max(64, 64 * Kp)), "timer")
+    _lib.check(lib.fs_timer_enable(ctx, max(64, 96 * Kp)), "timer")
     for k in range(Kp):
         dt_k = clock.next(a.particle_qd)
         evp[k][0].record()
@@ -748,16 +784,17 @@ def run_ours(args):
     passes = {}
     for p in range(npass):
         if cnt[p]:
-            name = lib.fs_pass_name(p).decode()
-            passes[name] = dict(ms_total=round(ms[p], 4), launches=int(cnt[p]), ms_avg=round(ms[p] / cnt[p], 5))
+            pname = lib.fs_pass_name(p).decode()
+            passes[pname] = dict(ms_total=round(ms[p], 4), launches=int(cnt[p]), ms_avg=round(ms[p] / cnt[p], 5))
     dom = max(passes, key=lambda k: passes[k]["ms_total"])
     peak, peak_kind = measured_peak()
     bpl = B_ALG.get(dom, 0) * n
     achieved = bpl / (passes[dom]["ms_avg"] * 1e-3) / 1e9
+    traffic = TRAFFIC_PER_PARTICLE.get(dom)
     roofline = dict(bound="hbm", kernel=dom, achieved=round(achieved, 1), peak=peak, unit="GB/s",
                     frac=round(achieved / peak, 4), peak_source=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                    traffic=(round(TRAFFIC_PER_PARTICLE[dom] * n) if dom in TRAFFIC_PER_PARTICLE else None),
-                    bytes_per_launch=bpl,
+                    traffic=(round(traffic * n) if traffic is not None else None),
+                    traffic_source=TRAFFIC_SOURCE.get(dom), bytes_per_launch=bpl,
                     share_of_step=round(passes[dom]["ms_total"] / max(instrumented_ms, 1e-9), 3))
     if dom in WARP_INST_PER_PARTICLE:
         inst = WARP_INST_PER_PARTICLE[dom] * n
@@ -767,7 +804,9 @@ def run_ours(args):
         roofline["issue"] = dict(kernel=dom, warp_instructions_per_launch=round(inst),
                                  achieved_warp_inst_per_s=round(rate), peak_warp_inst_per_s=round(peak_inst),
                                  frac=round(rate / peak_inst, 4), sm_mhz=mhz,
-                                 source="warp instructions per particle from the committed ncu capture")
+                                 source="warp instructions per particle from the committed ncu capture"
+                                 + ("" if name.startswith("pbf") or name.startswith("dfsph") or name.endswith("524k")
+                                    else " of the 524,288-particle lattice, scaled by the particle count"))
     bytes_per_step = sum(B_ALG.get(k, 0) * n * v["launches"] for k, v in passes.items()) / Kp
     gbs = bytes_per_step / (step_ms / K * 1e-3) / 1e9
     step_roofline = dict(algorithmic_bytes_per_step=bytes_per_step, achieved_gbs=round(gbs, 1),
@@ -799,44 +838,65 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
     e2e_value = world * n * Ke / (float(t_e2e.item()) * 1e-3)
+    rec = dict(value=round(value, 1), unit="particle-steps/s", steps=K, warmup=warmup,
+               ms_per_step=round(total_ms / K, 5), desc=desc, tuning=tuning,
+               e2e=dict(value=round(e2e_value, 1), unit="particle-steps/s", h2d_bytes_per_step=2 * n * 12,
+                        d2h_bytes_per_step=2 * n * 12, steps=Ke,
+                        path=f"host particle_q/qd (pinned) -> {type(solver).__name__}.step -> host"),
+               gpu_launches=int(launches), roofline=roofline, step_roofline=step_roofline, passes=passes,
+               passes_steps=Kp, passes_ms_per_step=round(instrumented_ms / Kp, 5), timer_dropped=int(dropped.value),
+               clocks=clk)
+    if iterations is not None:
+        rec["iterations_last_timed_step"] = iterations
+    del model, solver, a, b, s_in, s_out
+    torch.cuda.empty_cache()
+    if cpu_baseline:
+        rec["cpu_baseline"] = time_cpu_baseline(name, max_seconds=args.cpu_seconds)
+    return rec
 
-    # ---- secondary workloads (same timing rules and step count), N=1 only
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    if args.only:  # one secondary workload by itself (profiling); prints its record, not the bench line
+        if args.only == "adjoint":
+            rec = time_adjoint(dev, flush, reps=1)
+        elif args.only == "frames":
+            rec = [time_frame_loop(dev, flush), time_frame_loop(dev, flush, target=50000, frames=3),
+                   time_frame_loop(dev, flush, frames=3, method="dfsph")]
+        elif args.only == "metrics":
+            rec = time_metrics(dev)
+        elif args.only == "separation":
+            rec = time_separation(dev, flush)
+        else:
+            rec = time_batched(args.only.split("_")[1], dev, flush, frames=1, warm=1)
+        print(json.dumps(dict(only=args.only, record=rec)), flush=True)
+        return
+
+    head = measure_workload(args.workload, dev, flush, args.steps, args.warmup, args, world=world, clocks_gpu=local)
+
+    # ---- secondary workloads (same timing rules and step counts), N=1 only
     secondary = {}
     if world == 1 and not args.no_secondary:
         for wl in ("dfsph_dam_401856", "wcsph_stress_4m", "pbf_dam_401856_scorr"):
             if wl == args.workload:
                 continue
-            m2, s2, dt2, n2, d2 = build_workload(wl, dev)
-            c2 = HarnessClock(d2["solver"].lower(), d2.get("spacing", 0.0))
-            if d2["solver"] == "WCSPH":
-                c2.next = lambda v: dt2
-            x0, x1 = m2.state(), m2.state()
-            if not args.no_autotune:
-                from fluid_simulation_b200.autotune import autotune, describe
-                d2["tuning"] = describe(autotune(s2, x0, c2.limit if c2.kind == "dfsph" else dt2))
-            for _ in range(3):
-                s2.step(x0, x1, None, None, c2.next(x0.particle_qd))
-                x0, x1 = x1, x0
-            torch.cuda.synchronize()
-            k2 = max(5, K)
-            tot = 0.0
-            for _ in range(k2):
-                dt_k = c2.next(x0.particle_qd)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                s2.step(x0, x1, None, None, dt_k)
-                e1.record()
-                x0, x1 = x1, x0
-                flush.zero_()
-                e1.synchronize()
-                tot += e0.elapsed_time(e1)
-            rec = dict(d2, value=round(n2 * k2 / (tot * 1e-3), 1), unit="particle-steps/s",
-                       ms_per_step=round(tot / k2, 4), steps=k2)
-            if wl.startswith("dfsph"):
-                rec["iterations_last_step"] = s2.last_iterations()
-            secondary[wl] = rec
-            del m2, s2, x0, x1
-            torch.cuda.empty_cache()
+            rec = measure_workload(wl, dev, flush, args.steps, args.warmup, args, clocks_gpu=local,
+                                   cpu_baseline=not args.no_cpu_baseline and wl != "pbf_dam_401856_scorr")
+            desc = rec.pop("desc")
+            secondary[wl] = dict(desc, **rec)
 
     if world == 1 and not args.no_secondary and not args.no_batched:
         for kind in ("pbf", "wcsph", "dfsph"):
@@ -852,25 +912,24 @@ def run_ours(args):
         secondary["batched_adjoint_wcsph_256"] = time_adjoint(dev, flush, batched=True)
 
     cpu = None
-    if world == 1 and not args.no_cpu_baseline and not args.workload.startswith("wcsph_stress"):
+    if world == 1 and not args.no_cpu_baseline:
         cpu = time_cpu_baseline(args.workload, max_seconds=args.cpu_seconds)
 
     if rank == 0:
+        desc = head["desc"]
         line = dict(
-            metric="particle-steps/s", value=round(value, 1), unit="particle-steps/s", n_gpus=world, steps=K,
-            warmup=args.warmup, ms_per_step=round(total_ms / K, 5), higher_is_better=True, scaling="weak",
-            vs_baseline=round(value / PUBLISHED_PBF, 3) if args.workload == "pbf_dam_401856" else None,
+            metric="particle-steps/s", value=head["value"], unit="particle-steps/s", n_gpus=world, steps=head["steps"],
+            warmup=args.warmup, ms_per_step=head["ms_per_step"], higher_is_better=True, scaling="weak",
+            vs_baseline=round(head["value"] / PUBLISHED_PBF, 3) if args.workload == "pbf_dam_401856" else None,
             dtype="f32", data="synthetic (reference dam-break scene generator, seeded)",
             config=dict(desc, l2="flushed between timed steps (512 MB write outside the events)",
-                        tuning=tuning,
+                        tuning=head["tuning"],
                         parallelism="replicas" if world > 1 else "single GPU",
                         grid="HashGrid(128,128,128), cell = h, truncating cell coordinates"),
-            e2e=dict(value=round(e2e_value, 1), unit="particle-steps/s", h2d_bytes_per_step=2 * n * 12,
-                     d2h_bytes_per_step=2 * n * 12, steps=Ke,
-                     path=f"host particle_q/qd (pinned) -> {type(solver).__name__}.step -> host"),
-            gpu_launches=int(launches), roofline=roofline, step_roofline=step_roofline, passes=passes,
-            passes_steps=Kp, passes_ms_per_step=round(instrumented_ms / Kp, 5),
-            timer_dropped=int(dropped.value), clocks=clk, cpu_baseline=cpu, secondary=secondary or None,
+            e2e=head["e2e"], gpu_launches=head["gpu_launches"], roofline=head["roofline"],
+            step_roofline=head["step_roofline"], passes=head["passes"], passes_steps=head["passes_steps"],
+            passes_ms_per_step=head["passes_ms_per_step"], timer_dropped=head["timer_dropped"],
+            clocks=head["clocks"], cpu_baseline=cpu, secondary=secondary or None,
         )
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -879,36 +938,44 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU path for this workload, which
+    here is the C++ restatement of the reference solver (the reference
+    itself needs warp-lang + newton, which cannot be installed on these
+    hosts), on all host threads.  Same workload, config, warm-up count and
+    substep count as the GPU arm: W warm-up substeps from the initial state,
+    then K timed ones; only if those would run past --reference-seconds does
+    it stop early, and then it times the first k of the K substeps (said in
+    the line)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    if args.workload.startswith("wcsph_stress"):
-        raise SystemExit("the reference arm covers the dam-break workloads")
-    kind, model, state, cfg, n = cpu_oracle_setup(args.workload)
     import oracle
+    kind, model, state, cfg, n, clock = cpu_oracle_setup(args.workload)
+    advance = oracle_stepper(kind)
     cores = oracle.num_threads(os.cpu_count() or 1)
-    step = {"pbf": oracle.pbf_step, "dfsph": oracle.dfsph_step}[kind]
-    clock = HarnessClock(kind, cfg["particle_length"])
-    for _ in range(min(args.warmup, 1)):
-        out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
-        state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+    warmup = max(args.warmup, 3)  # the GPU arm's floor
+    t_start = time.perf_counter()
+    for _ in range(warmup):
+        state = advance(model, state, cfg, clock.next(state["particle_qd"]))
     k = 0
     t0 = time.perf_counter()
-    while k < args.steps and (k == 0 or time.perf_counter() - t0 < args.cpu_seconds * 3):
-        out = step(model, state, cfg, clock.next(state["particle_qd"]))[0]
-        state = dict(particle_q=out["particle_q"], particle_qd=out["particle_qd"], sph={})
+    while k < args.steps and (k == 0 or time.perf_counter() - t_start < args.reference_seconds):
+        state = advance(model, state, cfg, clock.next(state["particle_qd"]))
         k += 1
     el = time.perf_counter() - t0
     value = n * k / el
-    sample = (f"{k} of the requested {args.steps} substeps of the full {n}-particle workload in {el:.1f} s, "
-              f"C++ restatement of the reference solver (the reference needs warp-lang + newton, not "
-              f"installable here), OpenMP {cores} threads")
+    window = (f"substeps {warmup + 1}-{warmup + k} (all {args.steps} requested)" if k == args.steps else
+              f"substeps {warmup + 1}-{warmup + k}, the first {k} of the {args.steps} requested (stopped at "
+              f"{args.reference_seconds:.0f} s)")
+    sample = (f"{window} of the full {n}-particle workload after {warmup} warm-up substeps, in {el:.1f} s; "
+              f"C++ restatement of the reference solver, OpenMP {cores} threads")
     print(json.dumps(dict(
         impl="reference", metric="particle-steps/s", value=round(value, 1), unit="particle-steps/s", n_gpus=0,
-        steps=k, warmup=min(args.warmup, 1), ms_per_step=round(el / k * 1e3, 3), higher_is_better=True,
-        scaling="weak", vs_baseline=None, dtype="f32", data="synthetic (reference dam-break scene generator)",
-        config=dict(workload=args.workload, particles=n, dt=SUBSTEP_DT[kind] if kind == "pbf" else
-                    "harness CFL: min(rest of frame, 1/240, 0.4 spacing / max|v|)"),
+        steps=k, warmup=warmup, ms_per_step=round(el / k * 1e3, 3), higher_is_better=True,
+        scaling="weak", vs_baseline=None, dtype="f32", data="synthetic (reference dam-break scene generator, seeded)",
+        config=dict(workload_desc(args.workload), l2="host run (no device cache to flush)", tuning=None,
+                    parallelism="host threads",
+                    grid="HashGrid(128,128,128), cell = h, truncating cell coordinates"),
         cpu_baseline=dict(value=round(value, 1), unit="particle-steps/s", cores=cores, kind="port", sample=sample),
         e2e=dict(value=round(value, 1), unit="particle-steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
     )), flush=True)
@@ -925,6 +992,8 @@ def main():
                              "pbf_dam_401856_scorr"])
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--reference-seconds", type=float, default=240.0,
+                    help="reference arm: stop the timed substeps early past this many seconds in all")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -933,7 +1002,7 @@ def main():
     ap.add_argument("--only", choices=["adjoint", "batched_pbf", "batched_wcsph", "batched_dfsph", "frames", "metrics", "separation"],
                     help="run one secondary workload alone (profiling); no bench line")
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
+    if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)

@@ -47,13 +47,40 @@ def oracle_model(x, prm):
                 sph=dict(particle_mask=np.zeros(n, np.int32), **prm))
 
 
-def tape_rollout(x, v, prm, steps, dt=DT):
-    """FP64 torch rollout; x, v, prm entries are float64 tensors (leaves)."""
+def tape_rollout(x, v, prm, steps, dt=DT, cfg=CFG, mass=MASS):
+    """FP64 torch rollout; x, v, prm entries are float64 tensors (leaves),
+    all on one device."""
     n = x.shape[0]
-    mass = torch.full((n,), float(np.float32(MASS)), dtype=torch.float64)  # the model stores float32 masses
-    g = torch.tensor(GRAVITY, dtype=torch.float64)
-    cfg = dict(CFG, h=H)
+    mass = torch.full((n,), float(np.float32(mass)), dtype=torch.float64, device=x.device)  # float32 in the model
+    g = torch.tensor(GRAVITY, dtype=torch.float64, device=x.device)
+    cfg = dict(cfg, h=cfg["smoothing_length_coff"] * cfg["particle_length"])
     for _ in range(steps):
         x, v = wcsph_tape.substep(x, v, mass, prm["stiffness"], prm["viscosity"], prm["rest_density"],
                                   prm["exponent"], prm["surface_tension"], g, cfg, dt)
     return x, v
+
+
+def active_column(target=50000, sigma=0.1, seed=21):
+    """The differentiable dam-break workload at full size with pressure and
+    viscosity acting: the reference scene make_scene(target) (50,232
+    particles for 50,000) in the reference tank at the reference WCSPH
+    defaults (B = 250 kPa, exponent 7, viscosity 1e-6, clamped EOS), with a
+    seeded N(0, sigma) initial velocity field.  Over 120 substeps at
+    dt = 0.25 h / (c0 + max|v0|) the velocity field compresses parts of the
+    column (pressure up to ~20 kPa, ~6 % of the particles above rest
+    density at the end), viscosity acts on the relative velocities, and no
+    particle reaches a wall (closest approach 1.8 cm; a wall contact would
+    make the loss discontinuous).  Returns (scene, cfg, prm, x0, v0, dt)."""
+    from fluid_simulation_b200.scene import make_scene
+    s = make_scene(target)
+    n = s.count
+    cfg = dict(particle_radius=s.radius, particle_length=s.spacing, smoothing_length_coff=2.0, bound_width=1.2,
+               bound_height=0.28, bound_length=0.6, boundary_damping=0.0, clamp_negative_pressure=True)
+    prm = dict(stiffness=np.full(n, 2.5e5, np.float32), viscosity=np.full(n, 1e-6, np.float32),
+               rest_density=np.full(n, 1000.0, np.float32), surface_tension=np.zeros(n, np.float32),
+               exponent=np.full(n, 7.0, np.float32))
+    x0 = s.positions
+    v0 = (np.random.default_rng(seed).normal(size=x0.shape) * sigma).astype(np.float32)
+    c0 = (2.5e5 * 7.0 / 1000.0) ** 0.5
+    dt = 0.25 * (2.0 * s.spacing) / (c0 + float(np.linalg.norm(v0, axis=1).max()))
+    return s, cfg, prm, x0, v0, dt

@@ -209,47 +209,74 @@ def test_gradients_match_fp64_finite_differences(case, cuda_device):
         assert abs(ad - fd) <= GTOL * abs(fd), (name, ad, fd)
 
 
-def test_dam_break_50k_gradients_match_finite_differences(cuda_device):
-    """The differentiable dam-break workload at full size: make_scene(50000)
-    (50,232 particles), 120 substeps at the acoustic dt, checkpoints every 10
-    substeps with every segment but the last replayed; FP64 central finite
-    differences of the oracle along 32 random unit directions of v0 (eps =
-    1e-4 m/s).  In these 26 ms the column falls freely (it starts 3 cm above
-    the floor and below rest density, so the clamped pressure stays zero and
-    all velocities stay equal): the stiffness, viscosity and rest-density
-    gradients are exactly zero, as the finite differences confirm.
-    The oracle needs about 2 s per FP64 rollout on 16 host threads, so the
-    default run checks 4 directions; FS_FD_DIRECTIONS=32 runs all 32."""
-    ndir = int(os.environ.get("FS_FD_DIRECTIONS", "4"))
-    s, cfg, prm, dt, _ = dam_case(50000)
+def test_active_column_50k_gradients(cuda_device):
+    """The differentiable workload at full size with pressure and viscosity
+    acting (adjoint_util.active_column: make_scene(50000), 50,232
+    particles, N(0, 0.1 m/s) initial velocities, 120 substeps, checkpoints
+    every 10 with every segment but the last replayed).
+
+    * Against the FP64 tape (autograd through the torch restatement, run on
+      the GPU in FP64): the gradients w.r.t. v0, stiffness, viscosity and
+      rest density within 1e-3 norm-relative; all non-zero.
+    * Against FP64 central differences of the oracle (directional: v0 along
+      random unit directions, each parameter field scaled by 1 +- eps).  The
+      clamped EOS makes the loss piecewise smooth: it has kinks wherever a
+      particle's density crosses rest density, so a difference quotient
+      carries an error of its own that shrinks only like eps.  It is taken
+      at eps = 1e-5 and 3e-5, and the adjoint must lie within
+      max(1e-3 |FD|, 2 |FD(1e-5) - FD(3e-5)|) of FD(1e-5).  The oracle
+      needs a few seconds per FP64 rollout, so the default run checks 2 v0
+      directions; FS_FD_DIRECTIONS=32 runs 32."""
+    from adjoint_util import active_column, tape_rollout
+    ndir = int(os.environ.get("FS_FD_DIRECTIONS", "2"))
+    s, cfg, prm, x0, v0, dt = active_column()
     steps = 120
-    x0 = s.positions
     n = len(x0)
-    v0 = np.zeros_like(x0)
     target = x0.astype(np.float64) + np.array([0.3, 0.0, 0.0])
-    tgt = torch.tensor(target, dtype=torch.float32, device=cuda_device)
 
     def loss(xT, vT):
-        return ((xT - tgt) ** 2).sum(1).mean()
+        return ((xT - torch.as_tensor(target, dtype=xT.dtype, device=xT.device)) ** 2).sum(1).mean()
 
     sim = diff_sim(x0, prm, cuda_device, k=10, cfg=cfg, dt=dt, mass=s.mass, record_bytes=0)
     g = gpu_grads(sim, x0, v0, prm, steps, loss, cuda_device)
+    del sim
+    # FP64 tape on the device
+    leaves = [torch.tensor(a, dtype=torch.float64, device=cuda_device, requires_grad=True)
+              for a in (x0, v0, prm["stiffness"], prm["viscosity"], prm["rest_density"])]
+    p = dict(stiffness=leaves[2], viscosity=leaves[3], rest_density=leaves[4],
+             exponent=torch.tensor(prm["exponent"], dtype=torch.float64, device=cuda_device),
+             surface_tension=torch.tensor(prm["surface_tension"], dtype=torch.float64, device=cuda_device))
+    xT, vT = tape_rollout(leaves[0], leaves[1], p, steps, dt=dt, cfg=cfg, mass=s.mass)
+    loss(xT, vT).backward()
+    want = [t.grad.cpu().numpy() for t in leaves]
+    del leaves, p, xT, vT
+    torch.cuda.empty_cache()
+    errs = {nm: rel_err(a, b) for nm, a, b in zip(NAMES, g, want)}
+    print("adjoint vs FP64 tape", errs)
+    assert all(e <= GTOL for e in errs.values()), errs
+    for k in (1, 2, 3, 4):
+        assert np.abs(want[k]).max() > 0, NAMES[k]
+    # FP64 central differences
     rng = np.random.default_rng(2)
-    eps = 1e-4
-    worst = 0.0
+    checks = []
+
+    def fd(make):
+        out = []
+        for eps in (1e-5, 3e-5):
+            (xp, vp, pp), (xm, vm, pm) = make(eps), make(-eps)
+            out.append((oracle_loss(xp, vp, pp, cfg, dt, steps, s.mass, target) -
+                        oracle_loss(xm, vm, pm, cfg, dt, steps, s.mass, target)) / (2 * eps))
+        return out
+
     for _ in range(ndir):
         d = rng.normal(size=(n, 3))
         d /= np.linalg.norm(d)
-        fd = (oracle_loss(x0, v0 + eps * d, prm, cfg, dt, steps, s.mass, target) -
-              oracle_loss(x0, v0 - eps * d, prm, cfg, dt, steps, s.mass, target)) / (2 * eps)
-        ad = float(np.sum(g[1] * d))
-        worst = max(worst, abs(ad - fd) / abs(fd))
-    print(f"worst relative error over {ndir} directions", worst)
-    assert worst <= GTOL
+        f1, f2 = fd(lambda e: (x0, v0 + e * d, prm))
+        checks.append(("v0", float(np.sum(g[1] * d)), f1, f2))
     for key, gi in (("stiffness", 2), ("viscosity", 3), ("rest_density", 4)):
-        hi = dict(prm, **{key: prm[key].astype(np.float64) * (1 + eps)})
-        lo = dict(prm, **{key: prm[key].astype(np.float64) * (1 - eps)})
-        fd = (oracle_loss(x0, v0, hi, cfg, dt, steps, s.mass, target) -
-              oracle_loss(x0, v0, lo, cfg, dt, steps, s.mass, target)) / (2 * eps)
-        assert float(np.abs(g[gi]).max()) == 0.0, key
-        assert abs(fd) <= 1e-9, (key, fd)
+        f1, f2 = fd(lambda e: (x0, v0, dict(prm, **{key: prm[key].astype(np.float64) * (1 + e)})))
+        checks.append((key, float(np.sum(g[gi] * prm[key])), f1, f2))
+    print("adjoint vs FP64 central differences (eps 1e-5, 3e-5)", checks)
+    for name, ad, f1, f2 in checks:
+        assert f1 != 0.0, name
+        assert abs(ad - f1) <= max(GTOL * abs(f1), 2.0 * abs(f1 - f2)), (name, ad, f1, f2)

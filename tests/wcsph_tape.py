@@ -2,7 +2,8 @@
 tape gradients: autograd through this plays the part of a wp.Tape through the
 reference kernels.  Each substep's neighbour set (pairs with r < h, found
 with a k-d tree at the substep's input positions) is held fixed, as in the
-hand-written adjoint.  Test infrastructure only (dense torch ops, small N)."""
+hand-written adjoint.  Test infrastructure only (dense torch ops; on a CUDA
+device when the inputs are there, which the 50k-particle rollout needs)."""
 
 import math
 
@@ -31,8 +32,8 @@ def cubic_gs(r, h):
 
 
 def walls(p, v, w, hh, l, damping):
-    lo = torch.tensor([-w, -hh, 0.0], dtype=p.dtype)
-    hi = torch.tensor([w, hh, 2.0 * l], dtype=p.dtype)
+    lo = torch.tensor([-w, -hh, 0.0], dtype=p.dtype, device=p.device)
+    hi = torch.tensor([w, hh, 2.0 * l], dtype=p.dtype, device=p.device)
     below = p < lo
     v = torch.where(below & (v < 0), v * damping, v)
     p = torch.where(below, lo.expand_as(p), p)
@@ -47,14 +48,15 @@ def substep(x, v, mass, stiffness, viscosity, rest_density, exponent, coh_st, g,
     bound_width/height/length, boundary_damping, clamp_negative_pressure."""
     h = cfg["h"]
     n = x.shape[0]
-    pairs = cKDTree(x.detach().numpy()).query_pairs(h, output_type="ndarray")
-    i = torch.as_tensor(np.concatenate([pairs[:, 0], pairs[:, 1]]), dtype=torch.long)
-    j = torch.as_tensor(np.concatenate([pairs[:, 1], pairs[:, 0]]), dtype=torch.long)
+    dev = x.device
+    pairs = cKDTree(x.detach().cpu().numpy()).query_pairs(h, output_type="ndarray")
+    i = torch.as_tensor(np.concatenate([pairs[:, 0], pairs[:, 1]]), dtype=torch.long, device=dev)
+    j = torch.as_tensor(np.concatenate([pairs[:, 1], pairs[:, 0]]), dtype=torch.long, device=dev)
     vol = mass / torch.clamp(rest_density, min=1e-6)
     mv = rest_density * vol
     d = x[i] - x[j]
     r = torch.sqrt((d * d).sum(1))
-    rho = mv * cubic_w(torch.zeros(n, dtype=x.dtype), h) + torch.zeros(n, dtype=x.dtype).index_add(
+    rho = mv * cubic_w(torch.zeros(n, dtype=x.dtype, device=dev), h) + torch.zeros(n, dtype=x.dtype, device=dev).index_add(
         0, i, mv[j] * cubic_w(r, h))
     p = stiffness * ((rho / torch.clamp(rest_density, min=1e-6)) ** exponent - 1.0)
     if cfg["clamp_negative_pressure"]:
@@ -67,7 +69,7 @@ def substep(x, v, mass, stiffness, viscosity, rest_density, exponent, coh_st, g,
     pres = -mass[j] * (P[i] + P[j])
     wc = (coh_st[i] / mass[i]) * mass[j] * cubic_w(torch.clamp(r, min=cfg["particle_radius"]), h)
     c = (visc + pres) * gs - wc
-    a = torch.zeros(n, 3, dtype=x.dtype).index_add(0, i, c[:, None] * d) + g
+    a = torch.zeros(n, 3, dtype=x.dtype, device=dev).index_add(0, i, c[:, None] * d) + g
     v1 = v + dt * a
     x1 = x + dt * v1
     x1, v1 = walls(x1, v1, cfg["bound_width"], cfg["bound_height"], cfg["bound_length"], cfg["boundary_damping"])
