@@ -18,6 +18,7 @@ FS_ERR_INVALID = 1
 FS_ERR_CUDA = 2
 FS_ERR_CAPACITY = 3
 FS_ERR_NOGRID = 4
+FS_ERR_NONFINITE = 5
 
 FS_STATUS_NONFINITE = 1
 FS_STATUS_GRID_OVERFLOW = 2

@@ -9,15 +9,21 @@
 //   2. scan:    exclusive prefix of the counts (tile sums, then a down-sweep
 //               in which each tile adds up the sums before it)
 //   3. scatter: tmp[off[key] + arrival] = i        (order inside a cell arbitrary)
-//   4. rank:    slot = off[key] + #{j in cell : j < i}; perm[slot] = i
-// Step 4 restores ascending original index inside each cell, which is the
+//   4. rank:    slot = off[key] + #{j in cell : j < i}; perm[slot] = i, for
+//               cells of up to kSmallCell particles
+//   5. crowded cells: one block sorts each cell's ids (fs_sort.cuh)
+// Steps 4-5 restore ascending original index inside each cell, which is the
 // order warp's stable radix sort produces, so results do not depend on the
-// order in which atomics were served.
+// order in which atomics were served; the work is O(N) at any occupancy.
+// Non-finite positions are not binned into a cell: they take the extra key
+// ncell (after every cell, visited by no query) and raise
+// FS_STATUS_NONFINITE, so a blown-up state costs no more than a finite one.
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 
 #include "fs_nbr.cuh"
+#include "fs_sort.cuh"
 
 namespace fs {
 
@@ -43,35 +49,46 @@ __device__ __forceinline__ void load_items(const int32_t* __restrict__ in, int64
 }
 
 __global__ void k_cell_keys(int64_t n, const float* __restrict__ x, float inv, int dim_x, int dim_y, int dim_z,
-                            int rounding, int32_t* __restrict__ key, int32_t* __restrict__ slot,
-                            int32_t* __restrict__ count, uint32_t* status, const fs_frame_clock* clock) {
+                            int rounding, int32_t discard, int32_t* __restrict__ key, int32_t* __restrict__ slot,
+                            int32_t* __restrict__ count, int32_t* big_n, uint32_t* status,
+                            const fs_frame_clock* clock) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || clock_idle(clock)) return;
+  if (i == 0) *big_n = 0;  // crowded cells of this build, counted by k_rank
   const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
-  if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(status, FS_STATUS_NONFINITE);
-  GridDev g;
-  g.dim_x = dim_x;
-  g.dim_y = dim_y;
-  g.dim_z = dim_z;
-  g.mask_x = g.mask_y = g.mask_z = -1;
-  const int k = phys_cell(g, to_cell(__fmul_rn(px, inv), rounding), to_cell(__fmul_rn(py, inv), rounding),
-                          to_cell(__fmul_rn(pz, inv), rounding));
+  int k = discard;
+  if (!(isfinite(px) && isfinite(py) && isfinite(pz))) {
+    atomicOr(status, FS_STATUS_NONFINITE);
+  } else {
+    GridDev g;
+    g.dim_x = dim_x;
+    g.dim_y = dim_y;
+    g.dim_z = dim_z;
+    g.mask_x = g.mask_y = g.mask_z = -1;
+    k = phys_cell(g, to_cell(__fmul_rn(px, inv), rounding), to_cell(__fmul_rn(py, inv), rounding),
+                  to_cell(__fmul_rn(pz, inv), rounding));
+  }
   key[i] = k;
   slot[i] = atomicAdd(count + k, 1);
 }
 
 // Batched contexts: key = (world, cell) as the world's base + its local cell.
 __global__ void k_cell_keys_worlds(int64_t n, const float* __restrict__ x, const int32_t* __restrict__ world,
-                                   const WorldDev* __restrict__ worlds, int nworlds, float inv,
+                                   const WorldDev* __restrict__ worlds, int nworlds, float inv, int32_t discard,
                                    int32_t* __restrict__ key, int32_t* __restrict__ slot,
-                                   int32_t* __restrict__ count, uint32_t* status, const fs_frame_clock* clock) {
+                                   int32_t* __restrict__ count, int32_t* big_n, uint32_t* status,
+                                   const fs_frame_clock* clock) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || clock_idle(clock)) return;
+  if (i == 0) *big_n = 0;
   const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
-  if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(status, FS_STATUS_NONFINITE);
   const int w = world[i];
   if (w < 0 || w >= nworlds) atomicOr(status, FS_STATUS_BOUNDS);
-  const int k = world_cell_key(worlds[world_index(w, nworlds)], inv, px, py, pz);
+  int k = discard;
+  if (!(isfinite(px) && isfinite(py) && isfinite(pz)))
+    atomicOr(status, FS_STATUS_NONFINITE);
+  else
+    k = world_cell_key(worlds[world_index(w, nworlds)], inv, px, py, pz);
   key[i] = k;
   slot[i] = atomicAdd(count + k, 1);
 }
@@ -170,16 +187,43 @@ __global__ void k_scatter(int64_t n, const int32_t* __restrict__ key, const int3
 
 __global__ void k_rank(int64_t n, const int32_t* __restrict__ key, const int32_t* __restrict__ off,
                        const int32_t* __restrict__ tmp, int32_t* __restrict__ perm, int32_t* __restrict__ skey,
-                       const fs_frame_clock* clock) {
+                       int32_t* big_cells, int32_t* big_n, const fs_frame_clock* clock) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n || clock_idle(clock)) return;
   const int32_t i = tmp[s];
   const int32_t c = key[i];
   const int32_t a = off[c], b = off[c + 1];
+  if (b - a > kSmallCell) {  // crowded: sorted by k_big_sort
+    if (s == a) big_cells[atomicAdd(big_n, 1)] = c;
+    return;
+  }
   int32_t rank = 0;
   for (int32_t t = a; t < b; ++t) rank += tmp[t] < i ? 1 : 0;
   perm[a + rank] = i;
   skey[a + rank] = c;
+}
+
+// The crowded cells listed by k_rank, one block each (grid-stride over the
+// list): ids sorted ascending, then perm / skey written.
+__global__ void __launch_bounds__(kSortThreads) k_big_sort(int64_t n, const int32_t* __restrict__ off,
+                                                           int32_t* tmp, int32_t* perm, int32_t* skey,
+                                                           const int32_t* __restrict__ big_cells,
+                                                           const int32_t* __restrict__ big_n,
+                                                           const fs_frame_clock* clock) {
+  extern __shared__ int32_t sort_smem[];
+  if (clock_idle(clock)) return;
+  const int nbig = *big_n;
+  const int bits = id_bits(n);
+  for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+    const int32_t c = big_cells[b];
+    const int32_t a = off[c], len = off[c + 1] - a;
+    int32_t* sorted = block_sort_ids(tmp + a, perm + a, len, bits, sort_smem);
+    for (int k = threadIdx.x; k < len; k += blockDim.x) {
+      perm[a + k] = sorted[k];  // same element when sorted == perm + a
+      skey[a + k] = c;
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void k_tables(int64_t n, int64_t ncell, const int32_t* __restrict__ perm, const int32_t* __restrict__ key,
@@ -215,6 +259,8 @@ __global__ void k_candidates(GridDev g, const float* __restrict__ q, const int32
 }  // namespace
 
 int scan_blocks(int64_t m) { return (int)((m + kScanTile - 1) / kScanTile); }
+
+constexpr int kBigSortBlocks = 148;  // one per SM
 
 NbrList nbr_list(const fs_context* c) {
   NbrList L;
@@ -253,24 +299,32 @@ int grid_build(fs_context* c, const float* x, int64_t n, float radius, cudaStrea
   if (n > c->capacity) return set_error(FS_ERR_CAPACITY, "grid_build: n=%lld > capacity=%lld", (long long)n,
                                         (long long)c->capacity);
   const float inv = 1.0f / radius;
-  PassScope ps_(c, P_GRID, st, n > 0 ? 5 : 2);
-  int rc = check_cuda(cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * c->ncell, st), "memset cell counts");
+  PassScope ps_(c, P_GRID, st, n > 0 ? 6 : 2);
+  // ncell + 1 buckets: the cells, then the non-finite positions
+  const int64_t nbucket = c->ncell + 1;
+  const int32_t discard = (int32_t)c->ncell;
+  int rc = check_cuda(cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * nbucket, st), "memset cell counts");
   if (rc) return rc;
   // a new grid invalidates recorded neighbour lists
   rc = check_cuda(cudaMemsetAsync(c->nb_ctl, 0, sizeof(ListCtl), st), "memset list control");
   if (rc) return rc;
   if (n > 0 && c->worlds)
-    k_cell_keys_worlds<<<blocks_for(n), kBlock, 0, st>>>(n, x, world, c->worlds, c->nworlds, inv, c->key, c->slot,
-                                                         c->cell_count, c->status, clock);
+    k_cell_keys_worlds<<<blocks_for(n), kBlock, 0, st>>>(n, x, world, c->worlds, c->nworlds, inv, discard, c->key,
+                                                         c->slot, c->cell_count, c->big_n, c->status, clock);
   else if (n > 0)
     k_cell_keys<<<blocks_for(n), kBlock, 0, st>>>(n, x, inv, c->grid.dim_x, c->grid.dim_y, c->grid.dim_z,
-                                                   c->grid.rounding, c->key, c->slot, c->cell_count, c->status, clock);
-  const int nb = scan_blocks(c->ncell);
-  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, clock);
-  k_scan_down<<<nb, kScanThreads, 0, st>>>(c->cell_count, c->ncell, c->scan_part, c->cell_off, clock);
+                                                   c->grid.rounding, discard, c->key, c->slot, c->cell_count, c->big_n,
+                                                   c->status, clock);
+  const int nb = scan_blocks(nbucket);
+  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(c->cell_count, nbucket, c->scan_part, clock);
+  k_scan_down<<<nb, kScanThreads, 0, st>>>(c->cell_count, nbucket, c->scan_part, c->cell_off, clock);
   if (n > 0) {
     k_scatter<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->slot, c->cell_off, c->tmp_ids, clock);
-    k_rank<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->cell_off, c->tmp_ids, c->perm, c->skey, clock);
+    k_rank<<<blocks_for(n), kBlock, 0, st>>>(n, c->key, c->cell_off, c->tmp_ids, c->perm, c->skey, c->big_cells,
+                                             c->big_n, clock);
+    // a few blocks, each taking crowded cells from the list (none: they return at once)
+    k_big_sort<<<kBigSortBlocks, kSortThreads, kSortSmemBytes, st>>>(n, c->cell_off, c->tmp_ids, c->perm, c->skey,
+                                                                      c->big_cells, c->big_n, clock);
   }
   rc = launch_check("grid_build");
   if (rc) return rc;
@@ -329,7 +383,7 @@ int fs_context_create(fs_context** out, int64_t capacity, const fs_grid_config* 
       (grid->rounding != 0 && grid->rounding != 1))
     return set_error(FS_ERR_INVALID, "fs_context_create: bad arguments");
   const int64_t ncell = (int64_t)grid->dim_x * grid->dim_y * grid->dim_z;
-  if (ncell > (int64_t)kScanTile * 4096 || capacity > (int64_t)0x7fffffff)
+  if (ncell >= (int64_t)kScanTile * 4096 || capacity > (int64_t)0x7fffffff)
     return set_error(FS_ERR_INVALID, "fs_context_create: grid of %lld cells or capacity too large",
                      (long long)ncell);
   DeviceGuard dg(device);
@@ -366,7 +420,7 @@ int fs_context_create_worlds(fs_context** out, int64_t capacity, const fs_world_
     d.walls[2] = b.bound_length;
     d.base = (int32_t)(ncell < 0x7fffffff ? ncell : 0x7fffffff);
     ncell += cells;
-    if (ncell > (int64_t)kScanTile * 4096) {
+    if (ncell >= (int64_t)kScanTile * 4096) {
       delete[] host;
       return set_error(FS_ERR_INVALID, "fs_context_create_worlds: more than %lld cells in all",
                        (long long)kScanTile * 4096);
@@ -439,14 +493,15 @@ static int context_alloc(fs_context* c, int64_t capacity, int64_t ncell) {
   c->capacity = capacity;
   c->ncell = ncell;
   const int64_t cap = capacity > 0 ? capacity : 1;
-  const int nb = scan_blocks(ncell);
+  const int nb = scan_blocks(ncell + 1);
   const int rb = reduction_blocks(cap);
   struct A {
     void** p;
     size_t bytes;
   } allocs[] = {
       {(void**)&c->key, sizeof(int32_t) * cap},         {(void**)&c->slot, sizeof(int32_t) * cap},
-      {(void**)&c->cell_count, sizeof(int32_t) * ncell}, {(void**)&c->cell_off, sizeof(int32_t) * (ncell + 1)},
+      {(void**)&c->cell_count, sizeof(int32_t) * (ncell + 1)}, {(void**)&c->cell_off, sizeof(int32_t) * (ncell + 2)},
+      {(void**)&c->big_cells, sizeof(int32_t) * max_big_cells(cap)}, {(void**)&c->big_n, sizeof(int32_t)},
       {(void**)&c->tmp_ids, sizeof(int32_t) * cap},     {(void**)&c->perm, sizeof(int32_t) * cap},
       {(void**)&c->skey, sizeof(int32_t) * cap},
       {(void**)&c->scan_part, sizeof(int32_t) * (nb + 1)},
@@ -489,7 +544,7 @@ int fs_context_destroy(fs_context* c) {
   if (!c) return FS_OK;
   DeviceGuard dg(c->device);
   timer_free(c->timer);
-  void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
+  void* ps[] = {c->key, c->slot, c->cell_count, c->cell_off, c->big_cells, c->big_n, c->tmp_ids, c->perm, c->skey, c->scan_part, c->xs, c->xs2,
                 c->vs, c->vs2, c->mv, c->sc2, c->sc1, c->sc1b, c->krm, c->xo_tmp, c->vo_tmp, c->red_part, c->red_cnt,
                 c->dfsph, c->status, c->tile_stats, c->nb_idx, c->nb_cnt, c->nb_ctl, c->worlds, c->metrics,
                 c->dfsph_worlds, c->pbf_disp};

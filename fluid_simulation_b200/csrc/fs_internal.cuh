@@ -83,9 +83,11 @@ struct fs_context {
   // grid build
   int32_t* key = nullptr;        // [cap] cell key of original particle i
   int32_t* slot = nullptr;       // [cap] arrival slot inside the cell
-  int32_t* cell_count = nullptr; // [ncell]
-  int32_t* cell_off = nullptr;   // [ncell + 1]
+  int32_t* cell_count = nullptr; // [ncell + 1]; the last bucket holds non-finite positions
+  int32_t* cell_off = nullptr;   // [ncell + 2]
   int32_t* tmp_ids = nullptr;    // [cap] unordered-in-cell ids
+  int32_t* big_cells = nullptr;  // [max_big_cells(cap)] cells too crowded to rank in place
+  int32_t* big_n = nullptr;      // [1] how many
   int32_t* perm = nullptr;       // [cap] sorted slot -> original index
   int32_t* skey = nullptr;       // [cap] cell key of each sorted slot
   int32_t* scan_part = nullptr;  // [scan blocks + 1]

@@ -37,6 +37,7 @@ typedef struct fs_context fs_context;
 #define FS_ERR_CUDA 2      /* a CUDA runtime call failed (fs_last_error_string) */
 #define FS_ERR_CAPACITY 3  /* n exceeds the context capacity */
 #define FS_ERR_NOGRID 4    /* a pass needs a grid that was not built for this n */
+#define FS_ERR_NONFINITE 5 /* fs_wcsph_density_noalloc only: a position was not finite */
 
 /* device status word bits (sticky until fs_status_clear) */
 #define FS_STATUS_NONFINITE 1u      /* a non-finite position reached the grid build */
@@ -413,16 +414,19 @@ int fs_list_stats_enable(fs_context* ctx, int32_t on);
 
 /* ---- allocation-free density (no counterpart in the reference) ----------
  * For callers that cannot allocate device memory (hosts whose allocator
- * forbids cudaMalloc, plugins inside a runtime that owns all device memory,
- * work recorded into a CUDA graph): grid build + WCSPH density and EOS, the
- * results of fs_grid_build + fs_wcsph_density (up to summation order), in a
- * fixed scratch area compiled into the library (about 1 MB per GPU that loads
- * it, held until exit) instead of an fs_context.  At most
- * fs_noalloc_max_particles() particles; larger n returns FS_ERR_CAPACITY.
- * The first call on each device looks up the scratch address
- * (cudaGetSymbolAddress); make that call before any stream capture.  All
- * calls share the one scratch area: calls whose work overlaps on the GPU
- * (other streams, other host threads) race and give wrong results. */
+ * forbids cudaMalloc, plugins inside a runtime that owns all device memory):
+ * grid build + WCSPH density and EOS, the results of fs_grid_build +
+ * fs_wcsph_density (up to summation order), in a fixed scratch area compiled
+ * into the library (about 1 MB per GPU that loads it, held until exit)
+ * instead of an fs_context.  At most fs_noalloc_max_particles() particles;
+ * larger n returns FS_ERR_CAPACITY.  The scratch address is looked up
+ * (cudaGetSymbolAddress) on the first call in each CUDA context and cached
+ * under that context; make that first call before any stream capture.  The
+ * call waits for its stream: it reads back a status word and returns
+ * FS_ERR_NONFINITE when a position is not finite (that particle's density
+ * is 0 and it adds nothing to the others).  All calls share the one scratch
+ * area: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race and give wrong results. */
 int32_t fs_noalloc_max_particles(void);
 int fs_wcsph_density_noalloc(const fs_model* model, const float* x, float h, int32_t clamp_negative, float* rho,
                              float* pressure, fs_stream_t stream);
