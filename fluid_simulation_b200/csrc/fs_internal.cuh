@@ -101,7 +101,7 @@ struct fs_context {
   float2* sc2 = nullptr;  // per-slot scalar pair (rho, p) / (rho, factor)
   float* sc1 = nullptr;   // per-slot scalar (kappa / lambda)
   float* sc1b = nullptr;  // per-slot scalar (second)
-  float2* krm = nullptr;  // per-slot (kappa / rho, mass): the DFSPH correction's neighbour gather
+  float2* krm = nullptr;  // per-slot (kappa / rho, mass) for the DFSPH correction, (lambda, mass) for PBF's delta
   float* xo_tmp = nullptr;  // [cap*3] original-order scratch positions (PBF x_pred)
   float* vo_tmp = nullptr;  // [cap*3] original-order scratch velocities (PBF v_pred)
 

@@ -102,6 +102,8 @@ FS_DEV bool exact_lt_h(float dx, float dy, float dz, float h, float h2) {
 // 1.1 % after 500), and each overflowing particle rescans the grid in every
 // pass at those positions, its whole warp with it.
 constexpr int kNbMax = 192;
+// Entry offsets k * stride (k < kNbMax) fit 32 bits up to this stride (capacity).
+constexpr int64_t kListStride32Max = 0xffffffffLL / kNbMax;
 
 struct ListCtl {
   int32_t valid;  // lists recorded for the current grid and positions
@@ -118,34 +120,62 @@ struct NbrList {
 // Records the grid candidates of slot s with r^2 + w <= h2m (self included)
 // in visiting order; returns the active candidates other than s (the DFSPH
 // neighbour count, no distance test) when COUNT.
+//
+// A row range that fits in the list whatever it holds (n + its length <=
+// kNbMax) takes the short loop: no per-candidate capacity test, and the
+// entry offset is 32-bit when the list fits (stride <= kListStride32Max).
+// Other ranges take the checked loop.  Both record the same entries.
 template <bool COUNT>
 FS_DEV int record_list(const GridDev& g, const float4* __restrict__ xs, int s, float4 xi, float h, float h2m,
                        const NbrList& L) {
   int n = 0, ncand = 0;
-  int32_t* out = L.idx + s;  // entry n of slot s lives at out[n * stride]
+  int32_t* const col = L.idx + s;  // entry k of slot s lives at col[k * stride]
   const int64_t stride = L.stride;
-  auto test = [&](int t, float4 xj) {
-    if (COUNT) ncand += (t != s) ? (__float_as_int(xj.w) & PF_ACTIVE) : 0;
+  const bool off32 = stride <= kListStride32Max;  // uniform across the launch
+  const uint32_t stride32 = (uint32_t)stride;
+  auto r2_of = [&](float4 xj) {
     const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xj.w)));  // +inf for inactive
-    if (r2 <= h2m) {
-      if (n < kNbMax) {
-        *out = t;
-        out += stride;
-      }
+    return fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xj.w)));  // +inf for inactive
+  };
+  auto count = [&](int t, float4 xj) {
+    if (COUNT) ncand += (t != s) ? (__float_as_int(xj.w) & PF_ACTIVE) : 0;
+  };
+  auto checked = [&](int t, float4 xj) {
+    count(t, xj);
+    if (r2_of(xj) <= h2m) {
+      if (n < kNbMax) col[(int64_t)n * stride] = t;
       ++n;
     }
   };
   for_each_range(g, world_of(xi), xi.x, xi.y, xi.z, h, [&](int a, int e) {
     int t = a;
-    for (; t + 4 <= e; t += 4) {  // four independent loads in flight
-      const float4 x0 = __ldg(xs + t), x1 = __ldg(xs + t + 1), x2 = __ldg(xs + t + 2), x3 = __ldg(xs + t + 3);
-      test(t, x0);
-      test(t + 1, x1);
-      test(t + 2, x2);
-      test(t + 3, x3);
+    if (off32 && n + (e - a) <= kNbMax) {
+      uint32_t o = (uint32_t)n * stride32;
+      auto fast = [&](int tt, float4 xj) {
+        count(tt, xj);
+        const bool hit = r2_of(xj) <= h2m;
+        if (hit) col[o] = tt;
+        o += hit ? stride32 : 0u;
+        n += hit ? 1 : 0;
+      };
+      for (; t + 4 <= e; t += 4) {  // four independent loads in flight
+        const float4 x0 = __ldg(xs + t), x1 = __ldg(xs + t + 1), x2 = __ldg(xs + t + 2), x3 = __ldg(xs + t + 3);
+        fast(t, x0);
+        fast(t + 1, x1);
+        fast(t + 2, x2);
+        fast(t + 3, x3);
+      }
+      for (; t < e; ++t) fast(t, __ldg(xs + t));
+      return;
     }
-    for (; t < e; ++t) test(t, __ldg(xs + t));
+    for (; t + 4 <= e; t += 4) {
+      const float4 x0 = __ldg(xs + t), x1 = __ldg(xs + t + 1), x2 = __ldg(xs + t + 2), x3 = __ldg(xs + t + 3);
+      checked(t, x0);
+      checked(t + 1, x1);
+      checked(t + 2, x2);
+      checked(t + 3, x3);
+    }
+    for (; t < e; ++t) checked(t, __ldg(xs + t));
   });
   L.cnt[s] = n <= kNbMax ? n : kNbMax + 1;
   return ncand;
