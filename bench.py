@@ -63,13 +63,13 @@ B_ALG = {
 }
 PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 4090 (performance_summary.json)
 # DRAM bytes (read + write) per particle per launch, cold cache, from the
-# ncu capture of one PBF substep's four k_lambda launches at 401,856
-# particles (summary committed under profiles/): the first reuses the
-# density pass's lists and reads them back, 81.88 MB; the three scanning
-# ones 41.1-43.0 MB; their mean.
-TRAFFIC_PER_PARTICLE = {"pbf_lambda": 51.78e6 / 401856, "dfsph_rate": 68.17e6 / 401856,
-                        "dfsph_density_factor": 36.86e6 / 401856, "wcsph_density": 73.53e6 / 524288,
-                        "wcsph_force": 95.78e6 / 524288}
+# ncu captures summarised under profiles/: PBF lambda, the mean of one
+# substep's four launches at 401,856 particles (the first reuses the density
+# pass's lists and reads them back, 79.64 MB; the three scanning ones 38.2
+# MB each); WCSPH at 524,288 particles.
+TRAFFIC_PER_PARTICLE = {"pbf_lambda": 48.56e6 / 401856, "dfsph_rate": 68.17e6 / 401856,
+                        "dfsph_density_factor": 36.86e6 / 401856, "wcsph_density": 62.30e6 / 524288,
+                        "wcsph_force": 94.48e6 / 524288}
 TRAFFIC_SOURCE = {
     "pbf_lambda": "ncu, mean of one substep's 4 launches at 401,856 particles (profiles/pbf_dam_401856.md)",
     "dfsph_rate": "ncu, one launch at 401,856 particles (profiles/dfsph_dam_401856.md)",
@@ -79,13 +79,13 @@ TRAFFIC_SOURCE = {
 }
 # Warp instructions per particle per launch from the ncu captures of the
 # PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 38.21 M for the
-# reusing launch and 82.35 M for each scanning one; PBF delta: the mean of
+# reusing launch and 92.03 M for each scanning one; PBF delta: the mean of
 # its four launches).  The neighbour passes are bound by instruction issue, so the bench reports
 # the issue rate beside the HBM roofline.  Issue peak = 148 SMs x 4
 # schedulers x 1 warp instruction per cycle at the SM clock sampled during
 # the timed region.
-WARP_INST_PER_PARTICLE = {"pbf_lambda": 71.32e6 / 401856, "pbf_delta": 24.03e6 / 401856,
-                          "wcsph_density": 114.68e6 / 524288, "wcsph_force": 49.30e6 / 524288,
+WARP_INST_PER_PARTICLE = {"pbf_lambda": 78.58e6 / 401856, "pbf_delta": 24.03e6 / 401856,
+                          "wcsph_density": 126.16e6 / 524288, "wcsph_force": 49.30e6 / 524288,
                           "dfsph_density_factor": 92.02e6 / 401856, "dfsph_rate": 26.87e6 / 401856}
 FALLBACK_HBM_GBS = 6650.0
 SUBSTEP_DT = {"pbf": 1.0 / 240.0, "dfsph": 1.0 / 240.0}
@@ -603,6 +603,73 @@ def time_adjoint(dev, flush, batched=False, steps=120, k=10, reps=3):
     return rec
 
 
+# ------------------------------------------- WCSPH dam break, 60 frames ----
+def time_dam_60_frames(dev, target=10000, frames=60, cpu_seconds=20.0):
+    """The reference's CPU-runnable case: the WCSPH dam break of
+    make_scene(10000) (9,936 particles) for 60 display frames of 1/60 s
+    with the harness's CFL substeps (simulation.py:155-196), on the GPU
+    (DamBreakSimulation with the host loop, as the reference runs it, and
+    graph.DeviceFrameLoop) and with the CPU oracle on all host threads (the
+    harness restated over the oracle, tests/kat_util.OracleDamBreak) for as
+    many frames as fit in cpu_seconds.  Trajectories diverge chaotically,
+    so GPU and CPU are compared on kinetic energy and density statistics
+    after the frames the CPU ran.  Wall time per frame (the CFL readback
+    makes the host loop host-bound at this size)."""
+    import torch
+    import oracle
+    from fluid_simulation_b200.dam_break import DamBreakSimulation
+    from fluid_simulation_b200.graph import DeviceFrameLoop
+    from fluid_simulation_b200.scene import make_scene
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from kat_util import OracleDamBreak
+    s = make_scene(target)
+    n = s.count
+
+    def stats(x, v, rho):
+        ke = 0.5 * float(s.mass) * float((v.astype(np.float64) ** 2).sum())
+        return dict(kinetic_energy=ke, density_p99=float(np.percentile(rho, 99)), density_mean=float(rho.mean()),
+                    height_mean=float(x[:, 2].mean()))
+
+    out = dict(workload=f"wcsph_dam_{n}_60_frames", particles=n, frames=frames)
+    cores = oracle.num_threads(os.cpu_count() or 1)
+    cpu = OracleDamBreak(s, "wcsph")
+    t0 = time.perf_counter()
+    kc = 0
+    while kc < frames and (kc == 0 or time.perf_counter() - t0 < cpu_seconds):
+        cpu.step()
+        kc += 1
+    el = time.perf_counter() - t0
+    out["cpu_oracle"] = dict(frames=kc, ms_per_frame=round(el / kc * 1e3, 3), substeps=int(cpu.total_substeps),
+                             value=round(n * cpu.total_substeps / el, 1), unit="particle-steps/s (wall)", cores=cores,
+                             stats_at_its_last_frame=stats(cpu.x, cpu.v, cpu.sph["rho"]))
+    for name, make in (("gpu_host_loop", lambda: DamBreakSimulation(s, "wcsph", device=dev)),
+                       ("gpu_device_loop", lambda: DeviceFrameLoop(DamBreakSimulation(s, "wcsph", device=dev),
+                                                                   graph_substeps=64))):
+        run = make()
+        sim = run if isinstance(run, DamBreakSimulation) else run.sim
+        torch.cuda.synchronize()
+        el, at_kc = 0.0, None
+        for k in range(frames):
+            t0 = time.perf_counter()
+            run.step()
+            torch.cuda.synchronize()
+            el += time.perf_counter() - t0
+            if k + 1 == kc:
+                st = sim.state_0
+                at_kc = stats(st.particle_q.cpu().numpy(), st.particle_qd.cpu().numpy(), st.sph.rho.cpu().numpy())
+        st = sim.state_0
+        out[name] = dict(ms_per_frame=round(el / frames * 1e3, 3), substeps=int(sim.total_substeps),
+                         value=round(n * sim.total_substeps / el, 1), unit="particle-steps/s (wall)",
+                         stats_after_cpu_frames=at_kc,
+                         stats_after_60_frames=stats(st.particle_q.cpu().numpy(), st.particle_qd.cpu().numpy(),
+                                                     st.sph.rho.cpu().numpy()))
+        del run, sim
+    out["speedup_gpu_device_loop_vs_cpu"] = round(out["cpu_oracle"]["ms_per_frame"] /
+                                                  out["gpu_device_loop"]["ms_per_frame"], 1)
+    torch.cuda.empty_cache()
+    return out
+
+
 # -------------------------------------------------- harness frame loop ----
 def time_frame_loop(dev, flush, target=400000, frames=2, method="wcsph"):
     """WCSPH or DFSPH dam-break display frames (make_scene(target), CFL substeps of
@@ -851,7 +918,7 @@ def measure_workload(name, dev, flush, steps, warmup, args, world=1, clocks_gpu=
     del model, solver, a, b, s_in, s_out
     torch.cuda.empty_cache()
     if cpu_baseline:
-        rec["cpu_baseline"] = time_cpu_baseline(name, max_seconds=args.cpu_seconds)
+        rec["cpu_baseline"] = time_cpu_baseline(name, max_seconds=args.cpu_seconds, single_thread_seconds=0)
     return rec
 
 
@@ -902,6 +969,7 @@ def run_ours(args):
         for kind in ("pbf", "wcsph", "dfsph"):
             secondary[f"batched_{kind}_256"] = time_batched(kind, dev, flush)
     if world == 1 and not args.no_secondary:
+        secondary["wcsph_dam_9936_60_frames"] = time_dam_60_frames(dev)
         secondary["wcsph_dam_frames_401856"] = time_frame_loop(dev, flush)
         secondary["wcsph_dam_frames_50232"] = time_frame_loop(dev, flush, target=50000, frames=3)
         secondary["dfsph_dam_frames_401856"] = time_frame_loop(dev, flush, frames=3, method="dfsph")
