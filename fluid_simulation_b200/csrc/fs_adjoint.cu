@@ -5,7 +5,8 @@
 //
 // Forward, per dynamic particle i (j over active neighbours within h):
 //   rho_i = sum_j mv_j W(r_ij)                              (self included)
-//   p_i   = B_i ((rho_i / rho0_i)^gamma_i - 1)   [max(p, 0) when clamped]
+//   p_i   = B_i ((rho_i / rho0_i)^gamma_i - 1)   [max(p, 0) when clamped;
+//           its derivative is taken as 1 where p > 0 and 0 elsewhere]
 //   P_i   = p_i / max(rho_i^2, 1e-6),  R_i = 1 / max(rho_i, 1e-6)
 //   a_i   = g + sum_{j != i} c_ij d_ij,          d_ij = x_i - x_j,
 //   c_ij  = (visc_ij + pres_ij) gs(r) - coh_i m_j W(max(r, r_p))
@@ -246,7 +247,9 @@ __global__ void FS_NB_BOUNDS k_adj_force(AdjArgs a) {
     const float ratio = rho / rho0;
     const float pw = powf(ratio, gam);
     const float p_raw = B * (pw - 1.0f);
-    if (!(a.clamp && p_raw < 0.f) && pb != 0.f) {
+    // max(p, 0) has no derivative at p = 0; there the clamped side is taken
+    // (d/dp = 0), as for a ReLU: the pressure responds only where p > 0
+    if (!(a.clamp && !(p_raw > 0.f)) && pb != 0.f) {
       const float dp_dratio = B * gam * (ratio > 0.f ? pw / ratio : 0.f);
       rhob += pb * dp_dratio / rho0;
       if (a.gb_stiffness) a.gb_stiffness[i] += pb * (pw - 1.0f);

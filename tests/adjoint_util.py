@@ -84,3 +84,33 @@ def active_column(target=50000, sigma=0.1, seed=21):
     c0 = (2.5e5 * 7.0 / 1000.0) ** 0.5
     dt = 0.25 * (2.0 * s.spacing) / (c0 + float(np.linalg.norm(v0, axis=1).max()))
     return s, cfg, prm, x0, v0, dt
+
+
+def tape_along_trajectory(xs, vs, prm, seed_x, seed_v, dt, cfg, mass, pressure_on=None):
+    """Tape gradients along a given trajectory: xs[k], vs[k] (k = 0..K-1,
+    float64 or float32 tensors on one device) are the inputs of substep k as another
+    forward produced them.  Each substep is re-evaluated by the torch
+    restatement from its recorded input and differentiated alone; the
+    adjoints are chained from (seed_x, seed_v) = dL/d(x_K, v_K) back to
+    substep 0.  prm: stiffness, viscosity, rest_density (leaves of the same
+    dtype, gradients accumulate in .grad), exponent, surface_tension.  Returns
+    (dL/dx0, dL/dv0).  Unlike a tape rollout, the trajectory is the given
+    one, so this checks another forward's derivative; pressure_on[k] (bool
+    per particle, optional) fixes the clamped EOS's branch at substep k to
+    the one that forward took, so that an FP64 density a rounding away from
+    rest density does not switch a particle to the other side of the kink."""
+    dev, dtype = xs[0].device, xs[0].dtype
+    n = xs[0].shape[0]
+    m = torch.full((n,), float(np.float32(mass)), dtype=dtype, device=dev)
+    g = torch.tensor(GRAVITY, dtype=dtype, device=dev)
+    c = dict(cfg, h=cfg["smoothing_length_coff"] * cfg["particle_length"])
+    ax, av = seed_x, seed_v
+    for k in range(len(xs) - 1, -1, -1):
+        x = xs[k].clone().requires_grad_()
+        v = vs[k].clone().requires_grad_()
+        x1, v1 = wcsph_tape.substep(x, v, m, prm["stiffness"], prm["viscosity"], prm["rest_density"],
+                                    prm["exponent"], prm["surface_tension"], g, c, dt,
+                                    pressure_on=None if pressure_on is None else pressure_on[k])
+        torch.autograd.backward([x1, v1], [ax, av])
+        ax, av = x.grad, v.grad
+    return ax, av

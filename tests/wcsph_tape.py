@@ -43,9 +43,13 @@ def walls(p, v, w, hh, l, damping):
     return p, v
 
 
-def substep(x, v, mass, stiffness, viscosity, rest_density, exponent, coh_st, g, cfg, dt):
+def substep(x, v, mass, stiffness, viscosity, rest_density, exponent, coh_st, g, cfg, dt, pressure_on=None):
     """One substep, all particles active and dynamic.  cfg: h, particle_radius,
-    bound_width/height/length, boundary_damping, clamp_negative_pressure."""
+    bound_width/height/length, boundary_damping, clamp_negative_pressure.
+    pressure_on (bool per particle, optional): the clamp's branch taken from
+    another evaluation of the same state (p kept where True, 0 elsewhere), so
+    that the derivative follows that evaluation's side of the kink at rest
+    density."""
     h = cfg["h"]
     n = x.shape[0]
     dev = x.device
@@ -60,7 +64,8 @@ def substep(x, v, mass, stiffness, viscosity, rest_density, exponent, coh_st, g,
         0, i, mv[j] * cubic_w(r, h))
     p = stiffness * ((rho / torch.clamp(rest_density, min=1e-6)) ** exponent - 1.0)
     if cfg["clamp_negative_pressure"]:
-        p = torch.clamp(p, min=0.0)
+        # relu: derivative 0 at p = 0, the adjoint's convention for max(p, 0)
+        p = torch.relu(p) if pressure_on is None else torch.where(pressure_on, p, torch.zeros_like(p))
     P = p / torch.clamp(rho * rho, min=1e-6)
     R = 1.0 / torch.clamp(rho, min=1e-6)
     gs = cubic_gs(r, h)
