@@ -76,13 +76,15 @@ FS_DEV void r_and_inv(float r2, float& r, float& rinv) {
   r = r2 * rinv;
 }
 
-// `r < h` with r = sqrt(r^2) rounded as in a strict FP32 evaluation; only
-// the few pairs next to the support boundary pay for the exact square root.
-FS_DEV bool exact_lt_h(float dx, float dy, float dz, float h, float h2) {
-  const float r2 = dist2_rn(dx, dy, dz);
-  if (r2 < h2 * 0.999998f) return true;
-  if (r2 > h2 * 1.000002f) return false;
-  return sqrtf(r2) < h;
+// `r < h` with r = sqrt(r^2) rounded as in a strict FP32 evaluation, from
+// an r^2 the caller already has (any rounding within a few ulp, e.g. FMA
+// contracted): only the few pairs within 2e-6 of the support boundary
+// recompute r^2 with individually rounded operations and take the exact
+// square root.
+FS_DEV bool exact_lt_h(float r2_any, float dx, float dy, float dz, float h, float h2) {
+  if (r2_any < h2 * 0.999998f) return true;
+  if (r2_any > h2 * 1.000002f) return false;
+  return sqrtf(dist2_rn(dx, dy, dz)) < h;
 }
 
 

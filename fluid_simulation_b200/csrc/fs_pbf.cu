@@ -247,8 +247,8 @@ __global__ void FS_NB_BOUNDS_PBF k_lambda(LambdaArgs a) {
     visit_with<true, true>(a.g, a.xs, (int)s, xi, a.h, h2m, a.L, true, [&](int t) { return __ldg(&a.vs[t].w); },
                            [&](int t, float4 xj, const float& mj) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      if (t != (int)s && exact_lt_h(dx, dy, dz, a.h, K.h2)) ++cnt;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (t != (int)s && exact_lt_h(r2, dx, dy, dz, a.h, K.h2)) ++cnt;
       float r, rinv;
       r_and_inv(r2, r, rinv);
       rho = fmaf(mj, K.w_r2(r2), rho);

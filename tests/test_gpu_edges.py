@@ -10,7 +10,11 @@
     more than one particle), so the step raises; with a grid, rho = m W(0);
   - positions far outside the 128^3 hash range: cells alias, and the step
     still matches the oracle (candidates are filtered by distance);
-  - more particles than a context holds: a clear capacity error.
+  - more particles than a context holds: a clear capacity error;
+  - non-finite positions: the grid bins them apart and raises the status
+    word; every finite particle's step is bit-identical to the step of the
+    finite particles alone (in the reference a NaN candidate would turn its
+    neighbours' sums into NaN; its harness rejects such a state).
 """
 
 import ctypes as C
@@ -169,3 +173,25 @@ def test_more_particles_than_capacity_is_refused(cuda_device):
     rho = torch.zeros(len(x), device=cuda_device)
     rc = lib.fs_wcsph_density(grid._ctx, C.byref(ms), xt.data_ptr(), 0.02, 1, rho.data_ptr(), rho.data_ptr(), stream)
     assert rc == _lib.FS_ERR_NOGRID  # no grid was built for these points
+
+
+@pytest.mark.parametrize("kind", ["wcsph", "pbf"])
+def test_nonfinite_particles_leave_the_others_bit_identical(kind, cuda_device):
+    x, v = lattice(side=12, offset=(-0.05, -0.05, 0.1), seed=4)
+    bad = np.array([7, 300, 1000, 1500])
+    xb = x.copy()
+    xb[bad[0], 0], xb[bad[1], 1], xb[bad[2], 2], xb[bad[3]] = np.nan, np.inf, -np.inf, np.nan
+    ok = np.setdiff1d(np.arange(len(x)), bad)
+    outs = []
+    for xx, vv in ((xb, v), (x[ok], v[ok])):
+        m, solver, dt = make(kind, xx, vv, cuda_device)
+        a, b = m.state(), m.state()
+        solver.step(a, b, None, None, dt)
+        torch.cuda.synchronize()
+        outs.append((m, {"q": b.particle_q.cpu().numpy(), "qd": b.particle_qd.cpu().numpy(),
+                         "rho": b.sph.rho.cpu().numpy()}))
+    (m_bad, with_bad), (_, alone) = outs
+    for k in alone:
+        np.testing.assert_array_equal(with_bad[k][ok], alone[k], err_msg=k)
+    assert np.isfinite(with_bad["q"][ok]).all()
+    assert m_bad.particle_grid.status() & _lib.FS_STATUS_NONFINITE
