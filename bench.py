@@ -484,7 +484,7 @@ def time_metrics(dev, reps=20):
 
     t_dev, m_dev = wall(sim.metrics, reps)
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests"))
-    from numpy_metrics import numpy_frame_metrics  # the reference's way, as a checker
+    from numpy_metrics import numpy_frame_metrics  # the reference's way, to compare against
     t_host, m_host = wall(lambda: numpy_frame_metrics(sim), max(3, reps // 4))
     exact = ("speed_max", "height_min", "height_max", "density_min", "density_max", "density_p99", "pressure_min",
              "pressure_max")

@@ -5,8 +5,8 @@
 1.17.0's ``wp.HashGrid`` on the CPU.  This package wraps it with ctypes.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import it, and only as the checker (or the timed CPU
-baseline).  The product package never imports it.
+``bench.py`` may import it, and only to verify results (or as the timed
+CPU baseline).  The product package never imports it.
 
 Parity pin: the restatement is checked against golden vectors produced by
 running the reference's own solver source under a substitute Warp runtime

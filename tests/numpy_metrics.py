@@ -1,4 +1,4 @@
-"""Host-side checker for the device frame metrics.
+"""Host-side reference computation of the device frame metrics.
 
 The reference harness (examples/dam_break/simulation.py:198-225) copies the
 particle state to the host every frame and reduces it with numpy.  This
