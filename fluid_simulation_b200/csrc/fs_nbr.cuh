@@ -236,7 +236,12 @@ FS_DEV void visit(const GridDev& g, const float4* __restrict__ xs, int s, float4
 // as visit() calls pair(t, xj).  Only for lists recorded at the current
 // positions (every entry within h2m except the particle itself), where the
 // early load fetches nothing that visit() would not.  FRESH as in visit().
-template <bool WITH_SELF, bool FRESH = false, class Load, class Pair>
+// EVICT_FIRST: entries are loaded evict-first (ld.global.cs), leaving the
+// caches to the neighbours' data.  Measured faster for the PBF passes whose
+// lists at most one later pass reads again (delta, non-pressure, XSPH:
+// 1.304 -> 1.287 ms per substep at 401,856 particles); the DFSPH iteration
+// passes, which read the same lists 34 times a substep, were slower with it.
+template <bool WITH_SELF, bool FRESH = false, bool EVICT_FIRST = false, class Load, class Pair>
 FS_DEV void visit_with(const GridDev& g, const float4* __restrict__ xs, int s, float4 xi, float h, float h2m,
                        const NbrList& L, bool lists_ok, Load&& load, Pair&& pair) {
   const int n = lists_ok ? (FRESH ? L.cnt[s] : __ldg(L.cnt + s)) : kNbMax + 1;
@@ -247,7 +252,10 @@ FS_DEV void visit_with(const GridDev& g, const float4* __restrict__ xs, int s, f
   };
   if (use) {
     const int32_t* col = L.idx + s;
-    auto entry = [&](int k) { return FRESH ? col[(int64_t)k * L.stride] : __ldg(col + (int64_t)k * L.stride); };
+    auto entry = [&](int k) {
+      return FRESH ? col[(int64_t)k * L.stride]
+                   : (EVICT_FIRST ? __ldcs(col + (int64_t)k * L.stride) : __ldg(col + (int64_t)k * L.stride));
+    };
     int k = 0;
     for (; k + 3 < n; k += 4) {
       const int t0 = entry(k), t1 = entry(k + 1), t2 = entry(k + 2), t3 = entry(k + 3);

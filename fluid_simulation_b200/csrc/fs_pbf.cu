@@ -153,7 +153,7 @@ __global__ void FS_NB_BOUNDS_PBF k_accel_apply(AccelArgs a) {
     float ax = 0.f, ay = 0.f, az = 0.f;
     if (gamma != 0.f || mu != 0.f) {
       const bool lists_ok = a.use_lists && lists_usable(a.L);
-      visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+      visit_with<false, false, true>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
                         [&](int t) { return __ldg(a.vs + t); }, [&](int t, float4 xj, const float4& vj) {
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -316,7 +316,7 @@ __global__ void FS_NB_BOUNDS_PBF k_delta(DeltaArgs a) {
     const float inv_wdq = scorr ? 1.0f / a.w_dq : 0.f;
     float dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
     const bool lists_ok = a.use_lists && lists_usable(a.L);
-    visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+    visit_with<false, false, true>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
                       [&](int t) { return __ldg(a.lam_s + t); }, [&](int t, float4 xj, const float2& lj) {
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -380,7 +380,7 @@ __global__ void FS_NB_BOUNDS_PBF k_xsph_final(XsphArgs a) {
         const Poly6Spiky K(a.h);
         float cx = 0.f, cy = 0.f, cz = 0.f;
         const bool lists_ok = a.use_lists && lists_usable(a.L);
-        visit_with<false>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
+        visit_with<false, false, true>(a.g, a.xs, (int)s, xi, a.h, a.h * a.h * kSupportMargin, a.L, lists_ok,
                           [&](int t) { return __ldg(a.vel + t); }, [&](int t, float4 xj, const float4& vj) {
           const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
           // vj = (v, m / max(rho, 1e-6))
