@@ -67,7 +67,7 @@ PUBLISHED_PBF = 401856 * 4 / 0.06464700849610381   # particle-substeps/s, RTX 40
 # substep's four launches at 401,856 particles (the first reuses the density
 # pass's lists and reads them back, 79.64 MB; the three scanning ones 38.2
 # MB each); WCSPH at 524,288 particles.
-TRAFFIC_PER_PARTICLE = {"pbf_lambda": 48.56e6 / 401856, "dfsph_rate": 68.17e6 / 401856,
+TRAFFIC_PER_PARTICLE = {"pbf_lambda": 48.91e6 / 401856, "dfsph_rate": 68.17e6 / 401856,
                         "dfsph_density_factor": 36.86e6 / 401856, "wcsph_density": 62.30e6 / 524288,
                         "wcsph_force": 94.48e6 / 524288}
 TRAFFIC_SOURCE = {
@@ -78,13 +78,13 @@ TRAFFIC_SOURCE = {
     "wcsph_force": "ncu at 524,288 particles (profiles/wcsph_bcc_524k.md), scaled by the particle count",
 }
 # Warp instructions per particle per launch from the ncu captures of the
-# PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 38.21 M for the
-# reusing launch and 92.03 M for each scanning one; PBF delta: the mean of
-# its four launches).  The neighbour passes are bound by instruction issue, so the bench reports
+# PBF, WCSPH and DFSPH workloads (PBF lambda: the mean of 36.33 M for the
+# reusing launch and 90.41 M for each scanning one; PBF delta: the mean of
+# its captured launches).  The neighbour passes are bound by instruction issue, so the bench reports
 # the issue rate beside the HBM roofline.  Issue peak = 148 SMs x 4
 # schedulers x 1 warp instruction per cycle at the SM clock sampled during
 # the timed region.
-WARP_INST_PER_PARTICLE = {"pbf_lambda": 78.58e6 / 401856, "pbf_delta": 24.03e6 / 401856,
+WARP_INST_PER_PARTICLE = {"pbf_lambda": 76.89e6 / 401856, "pbf_delta": 24.32e6 / 401856,
                           "wcsph_density": 126.16e6 / 524288, "wcsph_force": 49.30e6 / 524288,
                           "dfsph_density_factor": 92.02e6 / 401856, "dfsph_rate": 26.87e6 / 401856}
 FALLBACK_HBM_GBS = 6650.0
