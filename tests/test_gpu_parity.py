@@ -161,3 +161,45 @@ def test_developed_dam_state(kind, cuda_device):
         _, _, info = oracle.dfsph_step(model, state, cfg, dt)
         it = solver.last_iterations()
         assert (it["rho_iterations"], it["vel_iterations"]) == (info["rho_iterations"], info["vel_iterations"])
+
+
+def test_wcsph_dam_signed_pressure(cuda_device):
+    """clamp_negative_pressure=False (solver_wcsph.py:156-157) at 401,856
+    particles: the tension side of the EOS acts too."""
+    s, model, state, common = dam_setup(400000)
+    cfg = dict(common, clamp_negative_pressure=False)
+    out, _, _ = run_step("wcsph", model, state, cfg, 1e-4)
+    compare("wcsph", out, model, state, cfg, 1e-4)
+
+
+def test_pbf_dam_grid_rebuilt_each_iteration(cuda_device):
+    """rebuild_grid_each_iteration=True (solver_pbf.py:858) at 401,856
+    particles: every constraint iteration builds the grid at the corrected
+    positions and scans it."""
+    s, model, state, common = dam_setup(400000)
+    cfg = dict(common, max_iterations=4, lambda_epsilon=100.0, min_neighbors_for_lambda=8, scorr_k=0.0,
+               scorr_n=4.0, scorr_q=0.3, max_delta_position=s.radius * 0.5, xsph_c=0.05,
+               rebuild_grid_each_iteration=True)
+    dt = 1.0 / 240.0
+    out, _, _ = run_step("pbf", model, state, cfg, dt)
+    compare("pbf", out, model, state, cfg, dt)
+
+
+def test_dfsph_dam_warm_start(cuda_device):
+    """warm_start=True at 401,856 particles: the step starts both solvers
+    from the kappa and kappa_v of state_in, here the ones a first GPU step
+    left; the second step is compared, with its iteration counts."""
+    s, model, state, common = dam_setup(400000)
+    cfg = dict(common, max_rho_iterations=5, max_vel_iterations=12, warm_start=False, eta_density=0.1,
+               eta_divergence=1e-4, max_kappa=1.0, max_kappa_v=100.0, min_neighbors_for_factor=15)
+    dt = 1.0 / 240.0
+    first, _, _ = run_step("dfsph", model, state, cfg, dt)
+    state2 = dict(particle_q=first["particle_q"], particle_qd=first["particle_qd"],
+                  sph=dict(kappa=first["sph"]["kappa"], kappa_v=first["sph"]["kappa_v"]))
+    assert np.abs(state2["sph"]["kappa"]).max() > 0 or np.abs(state2["sph"]["kappa_v"]).max() > 0
+    cfg = dict(cfg, warm_start=True)
+    _, _, info = oracle.dfsph_step(model, state2, cfg, dt)
+    out, solver, _ = run_step("dfsph", model, state2, cfg, dt)
+    it = solver.last_iterations()
+    compare("dfsph", out, model, state2, cfg, dt)
+    assert (it["rho_iterations"], it["vel_iterations"]) == (info["rho_iterations"], info["vel_iterations"])
