@@ -10,7 +10,9 @@ Checked here:
   - a batched frame replayed from a CUDA graph equals the eager steps;
   - a batched DFSPH substep takes its iteration decisions per world: every
     scene iterates as it would alone (same counts, same bits), and the scenes
-    chosen here stop after different numbers of iterations.
+    chosen here stop after different numbers of iterations;
+  - the whole 256-scene batch (6,190,898 particles), one PBF or DFSPH frame:
+    every scene bit-identical to the scene run alone.
 """
 
 import numpy as np
@@ -339,3 +341,56 @@ def test_batched_dfsph_frame_graph_equals_eager(cuda_device):
         res.append((out.particle_q.cpu().numpy(), solver.last_world_iterations()))
     assert np.array_equal(res[0][0], res[1][0])
     assert res[0][1] == res[1][1]
+
+
+@pytest.mark.parametrize("kind", ["pbf", "dfsph"])
+def test_full_batch_frame_equals_scenes_run_alone(kind, cuda_device):
+    """The whole 256-scene batch (6,190,898 particles, log-uniform scene
+    sizes 2,000-100,000) advanced one frame of 4 substeps as one model, from
+    seeded velocities: every scene's positions and velocities are bit-identical
+    to the same scene run alone with the plain solver (and, for DFSPH, so are
+    its iteration counts in the last substep)."""
+    from fluid_simulation_b200.batch import scene_model
+    b = make_batch()
+    v = velocities(b, seed=17, sigma=0.2)
+    common = dict(particle_radius=b.radius, particle_length=b.spacing, smoothing_length_coff=2.0,
+                  boundary_damping=0.0)
+    if kind == "pbf":
+        cls = SolverPBF
+        cfg = lambda w: SolverPBF.PbfConfig(max_iterations=4, lambda_epsilon=100.0, min_neighbors_for_lambda=8,
+                                            scorr_k=0.0, max_delta_position=b.radius * 0.5, xsph_c=0.05,
+                                            bound_width=w[0], bound_height=w[1], bound_length=w[2], **common)
+    else:
+        cls = SolverDFSPH
+        cfg = lambda w: SolverDFSPH.SphConfig(max_rho_iterations=5, max_vel_iterations=12, warm_start=False,
+                                              max_kappa=1.0, max_kappa_v=100.0, bound_width=w[0],
+                                              bound_height=w[1], bound_length=w[2], **common)
+    dt = 1.0 / 240.0
+    mb = batched_model(b, cls, device=cuda_device, v=v)
+    sb = cls(mb, cfg((1.0, 1.0, 1.0)))
+    a, c = mb.state(), mb.state()
+    for _ in range(4):
+        sb.step(a, c, None, None, dt)
+        a, c = c, a
+    torch.cuda.synchronize()
+    xb, vb = a.particle_q.cpu().numpy(), a.particle_qd.cpu().numpy()
+    per_world = sb.last_world_iterations() if kind == "dfsph" else None
+    del mb, sb, c
+    mismatched = []
+    for k, s in enumerate(b.scenes):
+        lo, hi = int(b.starts[k]), int(b.starts[k + 1])
+        m = scene_model(b, k, cls, device=cuda_device, v=v[lo:hi])
+        sv = cls(m, cfg(s.walls))
+        p, q = m.state(), m.state()
+        for _ in range(4):
+            sv.step(p, q, None, None, dt)
+            p, q = q, p
+        ok = np.array_equal(p.particle_q.cpu().numpy(), xb[lo:hi]) and \
+            np.array_equal(p.particle_qd.cpu().numpy(), vb[lo:hi])
+        if kind == "dfsph":
+            it, pw = sv.last_iterations(), per_world[k]
+            ok = ok and (it["rho_iterations"], it["vel_iterations"]) == (pw["rho_iterations"], pw["vel_iterations"])
+        if not ok:
+            mismatched.append(k)
+        del m, sv, p, q
+    assert not mismatched, mismatched
