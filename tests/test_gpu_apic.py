@@ -54,6 +54,21 @@ def test_dam_column_matches_oracle(cuda_device):
     assert np.array_equal(xg[flags == 0], x[flags == 0])            # inactive particles stay
 
 
+def test_full_size_dam_matches_oracle(cuda_device):
+    """The 401,856-particle dam-break scene, jittered by +-0.2 spacing, two
+    separation iterations (the harness default): bit-for-bit equal to the
+    oracle."""
+    s = make_scene(400000)
+    rng = np.random.default_rng(11)
+    x = (s.positions + rng.uniform(-0.2, 0.2, s.positions.shape) * s.spacing).astype(np.float32)
+    flags = np.ones(len(x), np.int32)
+    xg, dg, p = run(x, flags, s.radius, cuda_device, bound_lo=s.spec.bound_lo, bound_hi=s.spec.bound_hi)
+    xo, do = oracle.apic_separation(x, flags, p, "f32")
+    assert np.array_equal(xg, xo)
+    assert np.array_equal(dg, do)
+    assert np.count_nonzero(np.abs(xg - x).max(1)) > 0.1 * len(x)  # the pass acts
+
+
 def test_disabled_or_empty_is_a_no_op(cuda_device):
     x = np.zeros((0, 3), np.float32)
     m = model_from_arrays(x, x, 1.0, device=cuda_device, flags=np.zeros(0, np.int32), radius=0.01)
